@@ -1,0 +1,146 @@
+/*
+ * libldpcb200 — C ABI of the B200 AR4JA LDPC Monte Carlo engine.
+ *
+ * The reference runs its Monte Carlo hot path (channel -> layered Approximate-Min* decoding ->
+ * error tallies) inside one C++ function, run_ldpc_worker
+ * (engines/scalar_5w/ldpc_decoder_core.h:214-232), which its host harness drives one batch at a
+ * time (engines/scalar_5w/ldpc_sim_scalar.cpp:421-632) after parsing the parity-check matrix
+ * (ldpc_sim_scalar.cpp:116-269).  This header is the boundary that replaces that pair: a handle
+ * made from a parity-check matrix, a call that simulates one chunk of frames and returns the tallies
+ * the harness sums, and a call that decodes caller-supplied channel LLRs (the path of the
+ * reference's CPU steppers, tests/test_circulant_dma_stepper.cpp:861-990).
+ *
+ * Conventions: plain C types only; every function returns 0 on success or a negative errno-style
+ * code (LDPC_E*), never aborts, and leaves a message for ldpc_last_error() (per calling thread).
+ * The caller owns host buffers; the library owns device memory.  A handle is used by one thread at a
+ * time and issues its work on its own CUDA stream.
+ */
+#ifndef LDPCB200_H
+#define LDPCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDPCB200_ABI_VERSION 1
+
+/* Error codes (negative errno values). */
+#define LDPC_OK 0
+#define LDPC_EINVAL (-22)  /* bad argument */
+#define LDPC_ENOMEM (-12)  /* device or host allocation failed */
+#define LDPC_ENODEV (-19)  /* no usable CUDA device / kernel image */
+#define LDPC_ENOTSUP (-95) /* combination not built (e.g. a storage mode for a code shape) */
+#define LDPC_EIO (-5)      /* a CUDA call failed; see ldpc_last_error() */
+
+/* Message storage (engines/scalar_5w/ldpc_decoder_core.h:84-90, 476-520). */
+#define LDPC_STORE_BF16 0 /* L and r rounded to bf16 after every update: the reference numerics */
+#define LDPC_STORE_FP32 1 /* L and r in fp32 */
+#define LDPC_STORE_FP16 2 /* L in fp32, r rounded to IEEE fp16 */
+
+/* Check-node rule (ldpc_decoder_core.h:320-475; the reference's -n flag selects NMS). */
+#define LDPC_ALGO_AMIN 0 /* Approximate-Min* (Jones, MILCOM 2003) */
+#define LDPC_ALGO_NMS 1  /* normalised min-sum, alpha = 0.75 */
+
+/* Decoder family chosen for a matrix (ldpc_kernel_kind). */
+#define LDPC_KERNEL_QC 0      /* quasi-cyclic layered kernel (AR4JA structure detected) */
+#define LDPC_KERNEL_GENERAL 1 /* any matrix, rows in file order in conflict-free runs */
+
+typedef struct ldpc_handle ldpc_handle;
+
+/* A parity-check matrix: replaces the reference's ChinnMatrix (ldpc_sim_scalar.cpp:108-114).
+ * rows[m * max_check_deg + d] is the 0-based column of edge d of check m, in the order the matrix
+ * file lists it, -1 after the row's last edge.  The last n_punct columns are punctured. */
+typedef struct {
+    int32_t n_vars;        /* N */
+    int32_t n_checks;      /* M (checks) */
+    int32_t n_punct;       /* P */
+    int32_t max_check_deg; /* row stride of rows */
+    const int32_t* rows;   /* [n_checks][max_check_deg] */
+} ldpc_matrix;
+
+/* One chunk of simulation: replaces run_ldpc_worker's arguments (ldpc_decoder_core.h:214-232)
+ * and the per-batch runtime arguments of ldpc_sim_scalar.cpp:501-523.  Frame f of the chunk is
+ * global frame first_frame + f; its channel depends only on (seed, stream, global frame index). */
+typedef struct {
+    float mu;           /* channel LLR mean,  4 R Eb/N0       (ldpc_sim_scalar.cpp:351-355) */
+    float sigma;        /* channel LLR sigma, sqrt(8 R Eb/N0); 0 = noiseless (LLR = mu) */
+    uint64_t seed;      /* Philox key */
+    uint32_t stream;    /* Philox counter word 3: independent streams for one seed */
+    uint32_t reserved0;
+    uint64_t first_frame;
+    uint64_t n_frames;  /* frames in this chunk, >= 0 */
+    int32_t max_iter;   /* >= 0 */
+    int32_t storage;    /* LDPC_STORE_* */
+    int32_t algo;       /* LDPC_ALGO_* */
+    float l_max;        /* channel LLR clip (-L / -G), 0 = off  (ldpc_decoder_core.h:266-275) */
+    float r_max;        /* check message clip (-R), 0 = off      (:487) */
+    float l_post_max;   /* posterior clip (-V), 0 = off          (:492-495) */
+} ldpc_run_params;
+
+/* Tallies of one call: the per-worker stats of run_ldpc_worker (ldpc_decoder_core.h:580-585)
+ * summed over all frames of the chunk. */
+typedef struct {
+    uint64_t frames;
+    uint64_t bit_errors;   /* sign bits set over the first N-P positions, summed */
+    uint64_t frame_errors; /* frames with at least one such bit */
+    uint64_t iter_sum;     /* executed iterations, including the one that met the syndrome */
+    uint64_t unconverged;  /* frames whose syndrome still fails after decoding */
+    uint64_t max_iters;    /* largest iteration count of one frame */
+    float kernel_ms;       /* device time of the decode kernel (CUDA events on the handle's stream) */
+    float reserved1;
+} ldpc_tally;
+
+/* Replaces parse_chinn + the device setup of ldpc_sim_scalar.cpp:204-269, 319-392.  Copies the
+ * matrix; detects the quasi-cyclic AR4JA layer structure (12 layers of Z rows, degrees 3 and D)
+ * and selects the layered QC kernel, otherwise the general kernel.  device < 0 = current. */
+int ldpc_create(const ldpc_matrix* h, int device, ldpc_handle** out);
+
+/* Releases the handle and its device memory. */
+void ldpc_destroy(ldpc_handle* h);
+
+/* LDPC_KERNEL_QC or LDPC_KERNEL_GENERAL, or a negative error. */
+int ldpc_kernel_kind(const ldpc_handle* h);
+
+/* Simulates p->n_frames frames (channel generation, decoding, tallies) on the device; replaces one
+ * batch of ldpc_sim_scalar.cpp:421-589 (EnqueueMeshWorkload + ReadShard + host sums).  Blocks until
+ * the tallies are on the host. */
+int ldpc_run_chunk(ldpc_handle* h, const ldpc_run_params* p, ldpc_tally* out);
+
+/* Decodes n_frames caller-supplied frames: llr [n_frames][N-P] fp32 channel LLRs (host).  Uses
+ * p->max_iter, storage, algo and the clips (mu/sigma/seed ignored).  Outputs (each may be NULL):
+ * post [n_frames][N] final L as stored (bf16/fp16 values widened to float), iters, synd_fail (rows
+ * failing after decoding), bit_errors. */
+int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, int64_t n_frames,
+                    float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
+                    ldpc_tally* out);
+
+/* Writes the channel LLRs the simulation would decode for frames first_frame .. +n_frames-1
+ * (before storage rounding): llr [n_frames][N-P] (host).  For checking the channel. */
+int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);
+
+/* Iteration histogram of the last ldpc_run_chunk / ldpc_decode_llr: hist[i] = frames that used i
+ * iterations (the last bin also counts every larger value). */
+int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins);
+
+/* Launch shape override for the QC kernel (autotuning): rows per thread and frames per CTA; 0 =
+ * automatic.  Returns LDPC_ENOTSUP if that shape is not built for this code. */
+int ldpc_set_launch_shape(ldpc_handle* h, int rows_per_thread, int frames_per_cta);
+
+/* Number of kernel launches the handle issued since creation (for launch accounting). */
+int64_t ldpc_launch_count(const ldpc_handle* h);
+
+/* Copies the last error message of the calling thread into buf (NUL-terminated); returns its
+ * length. */
+int ldpc_last_error(char* buf, size_t len);
+
+/* LDPCB200_ABI_VERSION */
+int ldpc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LDPCB200_H */

@@ -1,0 +1,128 @@
+"""GPU parity: the CUDA kernels, called through the C ABI, against the reference's own decoder
+(golden fixtures from run_ldpc_worker) and against the CPU restatement in oracle/.
+
+Bar: bit-exact.  Posteriors, hard decisions, syndromes, iteration counts and tallies are integer or
+exactly-rounded values of the same operation sequence, so every comparison is equality of bit
+patterns (tolerance 0), in all three storage modes.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_frames, golden_matrix
+from ldpcb200 import ar4ja, capi
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def dec_r12k1(gpu):
+    c = ar4ja.make_code(1024, "1/2")
+    d = capi.Decoder.from_code(c, 0)
+    yield d
+    d.close()
+
+
+def test_qc_kernel_selected(dec_r12k1):
+    assert dec_r12k1.kind == capi.KERNEL_QC
+
+
+def _run_case(dec, case):
+    frames = golden_frames(case)
+    llr = np.stack([f[0] for f in frames])
+    want = np.stack([f[1] for f in frames])
+    p = dec.params(max_iter=case["max_iter"], storage="bf16",
+                   algo=capi.ALGO_NMS if case["nms"] else capi.ALGO_AMIN,
+                   l_max=case["l_max"], r_max=case["r_max"], l_post_max=case["l_post_max"])
+    post, it, sf, be, tal = dec.decode_llr(llr, p)
+    return frames, want, post, it, sf, be, tal
+
+
+@pytest.mark.parametrize("idx", range(23))
+def test_golden_reference_worker(golden, idx, gpu):
+    """Every fixture case: the GPU decoder fed the reference's own channel LLRs leaves exactly the
+    reference's bf16 posteriors, and its tallies equal run_ldpc_worker's stats."""
+    if idx >= len(golden["cases"]):
+        pytest.skip("no such case")
+    case = golden["cases"][idx]
+    rows, N, P = golden_matrix(golden, case["matrix"])
+    with capi.Decoder(rows, N, P, 0) as dec:
+        expect_kind = capi.KERNEL_GENERAL if case["matrix"] == "shipped" else capi.KERNEL_QC
+        assert dec.kind == expect_kind
+        frames, want, post, it, sf, be, tal = _run_case(dec, case)
+    assert np.array_equal(_bits(post), _bits(want)), f"posteriors differ in case {case['name']}"
+    # per pair: bit errors, frame errors, cw0 iterations (ldpc_decoder_core.h:580-585)
+    for p in range(case["stats"].shape[0]):
+        st = case["stats"][p]
+        k = slice(2 * p, min(2 * p + 2, len(frames)))
+        assert int(st[0]) == int(be[k].sum())
+        assert int(st[1]) == int((be[k] > 0).sum())
+        assert int(st[2]) == int(it[2 * p])
+    assert tal.frames == len(frames)
+    assert tal.bit_errors == int(be.sum()) and tal.frame_errors == int((be > 0).sum())
+    assert tal.iter_sum == int(it.sum())
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("ebn0", [0.75, 1.5, 2.5])
+def test_storage_modes_vs_oracle(dec_r12k1, storage, ebn0):
+    """FP32 / FP16 / BF16 message storage: bit-exact against the restatement with the same storage."""
+    c = ar4ja.make_code(1024, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, ebn0)
+    rng = np.random.default_rng(int(ebn0 * 100) + len(storage))
+    n = 24
+    llr = (mu + sigma * rng.standard_normal((n, c.n_tx))).astype(np.float32)
+    post, it, sf, be, tal = dec_r12k1.decode_llr(llr, max_iter=60, storage=storage)
+    mode = {"bf16": O.STORE_BF16, "fp32": O.STORE_FP32, "fp16": O.STORE_FP16}[storage]
+    opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=60)
+    assert np.array_equal(it, oit)
+    assert np.array_equal(be, obe)
+    assert np.array_equal(sf, osf)
+    assert np.array_equal(_bits(post), _bits(opost))
+
+
+def test_empty_batch(dec_r12k1):
+    post, it, sf, be, tal = dec_r12k1.decode_llr(np.zeros((0, 2048), np.float32), max_iter=10)
+    assert tal.frames == 0 and post.shape == (0, 2560)
+    r = dec_r12k1.run_chunk(dec_r12k1.params(mu=4.0, sigma=2.8, n_frames=0))
+    assert r.frames == 0
+
+
+def test_channel_matches_philox_oracle(dec_r12k1):
+    """The fused channel: Philox-4x32-10 counters (quad, frame, stream) under key seed, Box-Muller,
+    LLR = mu + sigma*n; compared with the double-precision restatement (tolerance: the GPU's fast
+    log/sin/cos, |diff| <= 2e-4 * (1 + |llr|))."""
+    mu, sigma = 2.5, 2.2
+    p = dec_r12k1.params(mu=mu, sigma=sigma, seed=0x1234_5678_9ABC, stream=3, first_frame=(1 << 33) + 5,
+                         n_frames=3)
+    g = dec_r12k1.channel_llr(p)
+    for f in range(3):
+        ref = O.philox_channel(0x1234_5678_9ABC, (1 << 33) + 5 + f, 2048, mu, sigma, stream=3)
+        assert np.all(np.abs(g[f] - ref) <= 2e-4 * (1 + np.abs(ref)))
+
+
+def test_sim_chunk_equals_decode_of_its_channel(dec_r12k1):
+    """run_chunk (channel fused in the kernel) tallies exactly what decode_llr gives on the same
+    frames' exported channel LLRs: the fused path and the external path are the same decoder."""
+    mu, sigma = capi.channel_mu_sigma(2560, 1536, 512, 1.25)
+    p = dec_r12k1.params(mu=mu, sigma=sigma, seed=7, first_frame=1000, n_frames=64, max_iter=100)
+    r = dec_r12k1.run_chunk(p)
+    llr = dec_r12k1.channel_llr(p)
+    _, it, sf, be, tal = dec_r12k1.decode_llr(llr, dec_r12k1.params(max_iter=100), want_post=False)
+    assert (r.frames, r.bit_errors, r.frame_errors, r.iter_sum) == \
+        (tal.frames, tal.bit_errors, tal.frame_errors, tal.iter_sum)
+
+
+def test_chunking_is_deterministic(dec_r12k1):
+    """Tallies depend only on (seed, frame range): one chunk equals the sum of its halves."""
+    mu, sigma = capi.channel_mu_sigma(2560, 1536, 512, 1.0)
+    whole = dec_r12k1.run_chunk(dec_r12k1.params(mu=mu, sigma=sigma, seed=11, first_frame=0, n_frames=2000))
+    a = dec_r12k1.run_chunk(dec_r12k1.params(mu=mu, sigma=sigma, seed=11, first_frame=0, n_frames=1200))
+    b = dec_r12k1.run_chunk(dec_r12k1.params(mu=mu, sigma=sigma, seed=11, first_frame=1200, n_frames=800))
+    assert whole.frames == 2000
+    for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged"):
+        assert getattr(whole, k) == getattr(a, k) + getattr(b, k)

@@ -1,0 +1,476 @@
+// Host side of libldpcb200: handles, structure detection, launch configuration, and the C ABI of
+// include/ldpcb200.h.  No CPU decoding path exists: every decode runs in a CUDA kernel, and a shape
+// that was not compiled is an error (LDPC_ENOTSUP).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ldpcb200.h"
+#include "ldpc_general.cuh"
+#include "ldpc_qc.cuh"
+#include "ldpc_registry.h"
+
+using namespace ldpcb200;
+
+// ----------------------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(LDPC_EIO, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ----------------------------------------------------------------------------- registry
+namespace ldpcb200 {
+static const QcTable* g_tables = nullptr;
+void register_qc_table(QcTable* t) {
+    t->next = g_tables;
+    g_tables = t;
+}
+const QcTable* qc_tables() { return g_tables; }
+}  // namespace ldpcb200
+
+static const void* find_qc(const QcKey& k) {
+    for (const QcTable* t = qc_tables(); t; t = t->next)
+        for (int i = 0; i < t->count; ++i)
+            if (t->entries[i].key == k) return t->entries[i].fn;
+    return nullptr;
+}
+
+// ----------------------------------------------------------------------------- handle
+struct ldpc_handle {
+    int device = 0;
+    int kind = LDPC_KERNEL_GENERAL;
+    int n_sm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // code
+    int N = 0, M = 0, P = 0, dmax = 0;
+    std::vector<int32_t> rows;  // [M][dmax]
+    // QC structure
+    int Z = 0, D = 0;
+    int32_t blk_off[QC_LAYERS][QC_DMAX] = {};
+    int32_t shift[QC_LAYERS][QC_DMAX] = {};
+    int force_R = 0, force_F = 0;
+    // general structure (device)
+    GeneralCode gen{};
+    // device scratch
+    unsigned long long* d_tally = nullptr;  // [TALLY_WORDS]
+    unsigned int* d_work = nullptr;
+    unsigned long long* d_hist = nullptr;
+    int hist_bins = 0;
+    float* d_llr = nullptr;
+    size_t llr_cap = 0;
+    float* d_post = nullptr;
+    size_t post_cap = 0;
+    int32_t* d_frame_out = nullptr;  // 3 * cap
+    size_t frame_cap = 0;
+    unsigned long long* h_tally = nullptr;  // pinned
+    int64_t launches = 0;
+};
+
+static int detect_qc(ldpc_handle* h) {
+    // 12 layers of Z rows; layers 0-3 of degree 3, layers 4-11 of one degree D; each edge of a layer
+    // is a circulant: column(j) = blk*Z + ((j + s) mod Z) for every row j of the layer, and the
+    // edges of a layer sit in distinct blocks (then the layer's rows share no column).
+    if (h->M % QC_LAYERS) return 0;
+    const int Z = h->M / QC_LAYERS;
+    if (Z < 32 || (Z & (Z - 1)) || h->N % Z || h->P % Z) return 0;
+    int D = -1;
+    for (int l = 0; l < QC_LAYERS; ++l) {
+        const int32_t* r0 = &h->rows[(size_t)(l * Z) * h->dmax];
+        int d = 0;
+        while (d < h->dmax && r0[d] >= 0) ++d;
+        if (l < 4 && d != QC_DEG_LOW) return 0;
+        if (l >= 4) {
+            if (D < 0) D = d;
+            if (d != D) return 0;
+        }
+        if (d > QC_DMAX) return 0;
+        std::vector<int> blks;
+        for (int e = 0; e < d; ++e) {
+            const int c0 = r0[e];
+            const int blk = c0 / Z, s = c0 % Z;
+            blks.push_back(blk);
+            for (int j = 0; j < Z; ++j) {
+                const int32_t* rj = &h->rows[(size_t)(l * Z + j) * h->dmax];
+                if (rj[e] != blk * Z + ((j + s) & (Z - 1))) return 0;
+            }
+            h->blk_off[l][e] = blk * Z;
+            h->shift[l][e] = s;
+        }
+        for (int j = 0; j < Z; ++j) {
+            const int32_t* rj = &h->rows[(size_t)(l * Z + j) * h->dmax];
+            if (d < h->dmax && rj[d] >= 0) return 0;
+        }
+        std::sort(blks.begin(), blks.end());
+        if (std::adjacent_find(blks.begin(), blks.end()) != blks.end()) return 0;
+    }
+    h->Z = Z;
+    h->D = D;
+    return 1;
+}
+
+static int ensure_cap(void** p, size_t* cap, size_t need) {
+    if (*cap >= need) return 0;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMalloc(p, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LDPC_ENOMEM, "cudaMalloc of %zu bytes failed", need);
+    }
+    *cap = need;
+    return 0;
+}
+
+extern "C" int ldpc_abi_version(void) { return LDPCB200_ABI_VERSION; }
+
+extern "C" int ldpc_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        strncpy(buf, g_err.c_str(), len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)g_err.size();
+}
+
+extern "C" void ldpc_destroy(ldpc_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_tally);
+    cudaFree(h->d_work);
+    cudaFree(h->d_hist);
+    cudaFree(h->d_llr);
+    cudaFree(h->d_post);
+    cudaFree(h->d_frame_out);
+    free_general(&h->gen);
+    if (h->h_tally) cudaFreeHost(h->h_tally);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+extern "C" int ldpc_create(const ldpc_matrix* m, int device, ldpc_handle** out) {
+    if (!out) return fail(LDPC_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!m || !m->rows) return fail(LDPC_EINVAL, "matrix is NULL");
+    if (m->n_vars <= 0 || m->n_checks <= 0 || m->max_check_deg <= 0 || m->max_check_deg > 64)
+        return fail(LDPC_EINVAL, "bad matrix dimensions N=%d M=%d max_check_deg=%d", m->n_vars,
+                    m->n_checks, m->max_check_deg);
+    if (m->n_punct < 0 || m->n_punct >= m->n_vars)
+        return fail(LDPC_EINVAL, "punctured count %d outside [0, N)", m->n_punct);
+    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i)
+        if (m->rows[i] >= m->n_vars || m->rows[i] < -1)
+            return fail(LDPC_EINVAL, "edge index out of bounds: row=%lld, col=%d",
+                        (long long)(i / m->max_check_deg) + 1, m->rows[i] + 1);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(LDPC_ENODEV, "no CUDA device");
+    }
+    ldpc_handle* h = new (std::nothrow) ldpc_handle();
+    if (!h) return fail(LDPC_ENOMEM, "host allocation failed");
+    if (device < 0) cudaGetDevice(&device);
+    h->device = device;
+    h->N = m->n_vars;
+    h->M = m->n_checks;
+    h->P = m->n_punct;
+    h->dmax = m->max_check_deg;
+    h->rows.assign(m->rows, m->rows + (size_t)h->M * h->dmax);
+    int rc = 0;
+    auto bail = [&](int code) { ldpc_destroy(h); return code; };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(LDPC_ENODEV, "cudaSetDevice(%d) failed", device));
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(LDPC_ENODEV, "no device properties"));
+    if (prop.major < 10) return bail(fail(LDPC_ENODEV, "device %s (sm_%d%d) is not sm_100", prop.name, prop.major, prop.minor));
+    h->n_sm = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
+        return bail(fail(LDPC_EIO, "stream/event creation failed"));
+    if (cudaMalloc(&h->d_tally, TALLY_WORDS * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&h->d_work, 64) != cudaSuccess ||
+        cudaMallocHost(&h->h_tally, TALLY_WORDS * sizeof(unsigned long long)) != cudaSuccess)
+        return bail(fail(LDPC_ENOMEM, "device allocation failed"));
+    h->hist_bins = 1024;
+    if (cudaMalloc(&h->d_hist, h->hist_bins * sizeof(unsigned long long)) != cudaSuccess)
+        return bail(fail(LDPC_ENOMEM, "device allocation failed"));
+    if (detect_qc(h) && h->N - h->P > 0 && ((h->N - h->P) % 32) == 0) {
+        h->kind = LDPC_KERNEL_QC;
+    } else {
+        h->kind = LDPC_KERNEL_GENERAL;
+        if ((rc = build_general(h->rows.data(), h->N, h->M, h->P, h->dmax, &h->gen, g_err)) != 0)
+            return bail(rc);
+    }
+    *out = h;
+    return 0;
+}
+
+extern "C" int ldpc_kernel_kind(const ldpc_handle* h) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    return h->kind;
+}
+
+extern "C" int64_t ldpc_launch_count(const ldpc_handle* h) { return h ? h->launches : -1; }
+
+extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int R, int F) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
+    if (R < 0 || F < 0 || F > QC_MAX_F) return fail(LDPC_EINVAL, "bad shape R=%d F=%d", R, F);
+    if (R || F) {
+        QcKey k{h->Z, h->D, R ? R : 1, F ? F : 1, LDPC_STORE_BF16, LDPC_ALGO_AMIN, 0, 0};
+        if (!find_qc(k)) {
+            k.mode = LDPC_STORE_FP32;
+            if (!find_qc(k)) return fail(LDPC_ENOTSUP, "shape R=%d F=%d not built for Z=%d D=%d", R, F, h->Z, h->D);
+        }
+    }
+    h->force_R = R;
+    h->force_F = F;
+    return 0;
+}
+
+static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    if (!p) return fail(LDPC_EINVAL, "params are NULL");
+    if (p->max_iter < 0 || p->max_iter > 1000000) return fail(LDPC_EINVAL, "max_iter %d out of range", p->max_iter);
+    if (p->storage < 0 || p->storage > 2) return fail(LDPC_EINVAL, "unknown storage mode %d", p->storage);
+    if (p->algo < 0 || p->algo > 1) return fail(LDPC_EINVAL, "unknown algorithm %d", p->algo);
+    if (!(p->l_max >= 0.0f) || !(p->r_max >= 0.0f) || !(p->l_post_max >= 0.0f))
+        return fail(LDPC_EINVAL, "clips must be >= 0");
+    if (!(p->sigma >= 0.0f) || p->mu != p->mu) return fail(LDPC_EINVAL, "bad channel mu/sigma");
+    return 0;
+}
+
+// Launch shape for the QC kernel: rows per thread R, frames per CTA F.
+static void qc_shape(const ldpc_handle* h, int mode, int* R, int* F) {
+    *R = h->force_R ? h->force_R : 1;
+    *F = h->force_F ? h->force_F : 1;
+    (void)mode;
+}
+
+static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
+                     const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
+    const bool clip = p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f;
+    int R, F;
+    qc_shape(h, p->storage, &R, &F);
+    QcKey key{h->Z, h->D, R, F, p->storage, p->algo, clip ? 1 : 0, ext ? 1 : 0};
+    const void* fn = find_qc(key);
+    if (!fn && (R != 1 || F != 1)) {  // fall back to the default shape of the same numerics
+        key.R = 1;
+        key.F = 1;
+        fn = find_qc(key);
+        R = F = 1;
+    }
+    if (!fn)
+        return fail(LDPC_ENOTSUP, "QC kernel Z=%d D=%d storage=%d algo=%d clip=%d ext=%d is not built", h->Z,
+                    h->D, p->storage, p->algo, (int)clip, (int)ext);
+    QcParams qp;
+    memset(&qp, 0, sizeof qp);
+    memcpy(qp.blk_off, h->blk_off, sizeof qp.blk_off);
+    memcpy(qp.shift, h->shift, sizeof qp.shift);
+    qp.n_vars = h->N;
+    qp.n_tx = h->N - h->P;
+    qp.max_iter = p->max_iter;
+    qp.mu = p->mu;
+    qp.sigma = p->sigma;
+    qp.l_max = p->l_max;
+    qp.r_max = p->r_max;
+    qp.l_post_max = p->l_post_max;
+    qp.seed_lo = (uint32_t)p->seed;
+    qp.seed_hi = (uint32_t)(p->seed >> 32);
+    qp.stream = p->stream;
+    qp.first_frame = first;
+    qp.n_frames = n;
+    qp.llr_in = d_llr;
+    qp.post_out = d_post;
+    qp.iters_out = d_it;
+    qp.synd_out = d_sf;
+    qp.be_out = d_be;
+    qp.tally = h->d_tally;
+    qp.hist = h->d_hist;
+    qp.hist_bins = h->hist_bins;
+    qp.work = h->d_work;
+    const int T = h->Z / R;
+    const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;
+    const size_t lstride = (size_t)((h->N + 7) & ~7);
+    const size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
+    if (smem > 48 * 1024) CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
+    if (per_sm <= 0) return fail(LDPC_ENOTSUP, "QC kernel does not fit on an SM (smem %zu)", smem);
+    const uint64_t want = (n + F - 1) / F;
+    const uint64_t grid = std::min<uint64_t>(want, (uint64_t)per_sm * h->n_sm);
+    if (grid == 0) return 0;
+    void* args[] = {&qp};
+    CU(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(T), args, smem, h->stream));
+    h->launches++;
+    return 0;
+}
+
+static int reset_counters(ldpc_handle* h) {
+    CU(cudaMemsetAsync(h->d_tally, 0, TALLY_WORDS * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(h->d_work, 0, 64, h->stream));
+    CU(cudaMemsetAsync(h->d_hist, 0, h->hist_bins * sizeof(unsigned long long), h->stream));
+    return 0;
+}
+
+static int read_tally(ldpc_handle* h, ldpc_tally* out) {
+    CU(cudaMemcpyAsync(h->h_tally, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (out) {
+        out->frames = h->h_tally[T_FRAMES];
+        out->bit_errors = h->h_tally[T_BIT_ERR];
+        out->frame_errors = h->h_tally[T_FRAME_ERR];
+        out->iter_sum = h->h_tally[T_ITER_SUM];
+        out->unconverged = h->h_tally[T_UNCONVERGED];
+        out->max_iters = h->h_tally[T_MAX_ITER];
+        out->kernel_ms = ms;
+        out->reserved1 = 0.0f;
+    }
+    return 0;
+}
+
+// Splits a request into launches of at most 2^31 frames (the kernel's claim counter is 32-bit).
+static constexpr uint64_t kMaxLaunchFrames = 1ull << 31;
+
+static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64_t n, const float* d_llr,
+                      float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
+    int rc;
+    if ((rc = reset_counters(h))) return rc;
+    CU(cudaEventRecord(h->ev0, h->stream));
+    for (uint64_t off = 0; off < n || (n == 0 && off == 0); off += kMaxLaunchFrames) {
+        if (n == 0) break;
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(kMaxLaunchFrames, n - off);
+        if (off) CU(cudaMemsetAsync(h->d_work, 0, 64, h->stream));
+        const float* llr = d_llr ? d_llr + off * (uint64_t)(h->N - h->P) : nullptr;
+        float* post = d_post ? d_post + off * (uint64_t)h->N : nullptr;
+        int32_t* it = d_it ? d_it + off : nullptr;
+        int32_t* sf = d_sf ? d_sf + off : nullptr;
+        int32_t* be = d_be ? d_be + off : nullptr;
+        if (h->kind == LDPC_KERNEL_QC)
+            rc = launch_qc(h, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be);
+        else
+            rc = launch_general(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be, h->d_tally,
+                                h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err);
+        if (rc) return rc;
+        if (h->kind != LDPC_KERNEL_QC) h->launches++;
+    }
+    CU(cudaEventRecord(h->ev1, h->stream));
+    CU(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int ldpc_run_chunk(ldpc_handle* h, const ldpc_run_params* p, ldpc_tally* out) {
+    int rc;
+    if ((rc = check_params(h, p))) return rc;
+    CU(cudaSetDevice(h->device));
+    if ((rc = run_frames(h, p, false, p->n_frames, nullptr, nullptr, nullptr, nullptr, nullptr))) return rc;
+    return read_tally(h, out);
+}
+
+extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, int64_t n,
+                               float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
+                               ldpc_tally* out) {
+    int rc;
+    if ((rc = check_params(h, p))) return rc;
+    if (n < 0) return fail(LDPC_EINVAL, "n_frames < 0");
+    if (n > 0 && !llr) return fail(LDPC_EINVAL, "llr is NULL");
+    CU(cudaSetDevice(h->device));
+    const size_t ntx = (size_t)(h->N - h->P);
+    const size_t nb = (size_t)n;
+    if (nb) {
+        if ((rc = ensure_cap((void**)&h->d_llr, &h->llr_cap, nb * ntx * sizeof(float)))) return rc;
+        if (post && (rc = ensure_cap((void**)&h->d_post, &h->post_cap, nb * h->N * sizeof(float)))) return rc;
+        if ((rc = ensure_cap((void**)&h->d_frame_out, &h->frame_cap, 3 * nb * sizeof(int32_t)))) return rc;
+        CU(cudaMemcpyAsync(h->d_llr, llr, nb * ntx * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    }
+    ldpc_run_params q = *p;
+    q.first_frame = 0;
+    q.n_frames = nb;
+    int32_t* d_it = h->d_frame_out;
+    int32_t* d_sf = d_it ? d_it + nb : nullptr;
+    int32_t* d_be = d_sf ? d_sf + nb : nullptr;
+    if ((rc = run_frames(h, &q, true, nb, h->d_llr, post ? h->d_post : nullptr, d_it, d_sf, d_be))) return rc;
+    if (nb) {
+        if (post) CU(cudaMemcpyAsync(post, h->d_post, nb * h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        if (iters) CU(cudaMemcpyAsync(iters, d_it, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        if (synd_fail) CU(cudaMemcpyAsync(synd_fail, d_sf, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        if (bit_errors) CU(cudaMemcpyAsync(bit_errors, d_be, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    return read_tally(h, out);
+}
+
+// Channel only: the Philox/Box-Muller LLRs of a range of frames, for checking the generator.
+__global__ void channel_kernel(float* out, int ntx, uint64_t first, uint64_t n, uint32_t seed_lo, uint32_t seed_hi,
+                               uint32_t stream, float mu, float sigma) {
+    const int nq = ntx >> 2;
+    const uint64_t total = n * (uint64_t)nq;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t f = i / nq;
+        const int qd = (int)(i % nq);
+        const uint64_t gf = first + f;
+        float v[4];
+        if (sigma > 0.0f) {
+            const U32x4 x = philox4x32_10(U32x4{(uint32_t)qd, (uint32_t)gf, (uint32_t)(gf >> 32), stream}, seed_lo, seed_hi);
+            box_muller(x.x, x.y, v[0], v[1]);
+            box_muller(x.z, x.w, v[2], v[3]);
+            for (int k = 0; k < 4; ++k) v[k] = __fmaf_rn(sigma, v[k], mu);
+        } else {
+            v[0] = v[1] = v[2] = v[3] = mu;
+        }
+        reinterpret_cast<float4*>(out + f * ntx)[qd] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+extern "C" int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr) {
+    int rc;
+    if ((rc = check_params(h, p))) return rc;
+    if (!llr && p->n_frames) return fail(LDPC_EINVAL, "llr is NULL");
+    const int ntx = h->N - h->P;
+    if (ntx % 4) return fail(LDPC_ENOTSUP, "channel export needs N-P divisible by 4");
+    CU(cudaSetDevice(h->device));
+    const size_t bytes = (size_t)p->n_frames * ntx * sizeof(float);
+    if (!bytes) return 0;
+    if ((rc = ensure_cap((void**)&h->d_llr, &h->llr_cap, bytes))) return rc;
+    channel_kernel<<<h->n_sm * 8, 256, 0, h->stream>>>(h->d_llr, ntx, p->first_frame, p->n_frames, (uint32_t)p->seed,
+                                                       (uint32_t)(p->seed >> 32), p->stream, p->mu, p->sigma);
+    h->launches++;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(llr, h->d_llr, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+extern "C" int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins) {
+    if (!h || !hist || n_bins <= 0) return fail(LDPC_EINVAL, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    std::vector<unsigned long long> tmp(h->hist_bins);
+    CU(cudaMemcpyAsync(tmp.data(), h->d_hist, h->hist_bins * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < n_bins; ++i) hist[i] = 0;
+    for (int i = 0; i < h->hist_bins; ++i) hist[std::min(i, n_bins - 1)] += tmp[i];
+    return 0;
+}

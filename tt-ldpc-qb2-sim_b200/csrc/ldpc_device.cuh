@@ -1,0 +1,71 @@
+// Device-side building blocks of the AR4JA Monte Carlo path (sm_100a).
+//
+//   * Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+//     SC'11): a counter-based generator, so frame f's channel depends only on (seed, f) and any
+//     chunk of frames can be regenerated independently (replaces the reference's per-core
+//     xoshiro128+ streams, engines/scalar_5w/ldpc_decoder_core.h:26-65).
+//   * Box-Muller AWGN and BPSK LLR formation: LLR = mu + sigma*n with mu = 4R Eb/N0,
+//     sigma = sqrt(8R Eb/N0) (engines/scalar_5w/ldpc_sim_scalar.cpp:351-355).
+//   * The Approximate-Min* step and storage rounding of the reference's scalar decoder
+//     (engines/scalar_5w/ldpc_decoder_core.h:84-90, 154-201).  Every multiply and add of the decoder
+//     is an explicit round-to-nearest intrinsic so the compiler never fuses them into an FMA: the
+//     reference rounds after each operation and the results must match it bit for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace ldpcb200 {
+
+enum Storage : int { STORE_BF16 = 0, STORE_FP32 = 1, STORE_FP16 = 2 };
+enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1 };
+
+// ------------------------------------------------------------------ Philox-4x32-10
+struct U32x4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U32x4 philox4x32_10(U32x4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = U32x4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    }
+    return c;
+}
+
+// Two uniforms -> two standard normals.  u1 = x0*2^-32 + 2^-33 lies in (0, 1]; the angle is
+// 2*pi*(x1*2^-32) - pi in [-pi, pi), the range where the fast hardware sine/cosine are accurate.
+__device__ __forceinline__ void box_muller(uint32_t x0, uint32_t x1, float& n0, float& n1) {
+    const float u1 = __fmaf_rn(__uint2float_rn(x0), 2.3283064365386963e-10f, 1.1641532182693481e-10f);
+    const float a = __fmaf_rn(__uint2float_rn(x1), 1.4629180792671596e-09f, -3.14159265358979f);
+    const float rad = __fsqrt_rn(-2.0f * __logf(u1));
+    float s, c;
+    __sincosf(a, &s, &c);
+    n0 = rad * c;
+    n1 = rad * s;
+}
+
+// ------------------------------------------------------------------ storage rounding
+__device__ __forceinline__ float bf16_round(float x) {  // fp32_to_bf16, RNE (ldpc_decoder_core.h:84-90)
+    return __bfloat162float(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ float fp16_round_sat(float x) {  // IEEE fp16 RNE, saturated at 65504
+    return __half2float(__float2half_rn(fminf(fmaxf(x, -65504.0f), 65504.0f)));
+}
+
+// ------------------------------------------------------------------ Approximate-Min*
+// min*(m, a) = max(min(m, a) - g(|m - a|), 0), g piecewise linear (ldpc_decoder_core.h:186-190).
+// With m = +inf the step returns a exactly, which lets the chain start from +inf instead of from the
+// first non-argmin edge (the reference's m_others = |q[first]|, :180-181).
+__device__ __forceinline__ float amin_step(float m, float a) {
+    const float diff = fabsf(__fsub_rn(m, a));
+    const float cur = fminf(m, a);
+    const float c1 = __fsub_rn(0.69315f, __fmul_rn(0.40f, diff));
+    const float c2 = __fsub_rn(0.49315f, __fmul_rn(0.328f, __fsub_rn(diff, 0.5f)));
+    float corr = diff < 0.5f ? c1 : c2;
+    corr = diff >= 2.0f ? 0.0f : corr;
+    return fmaxf(__fsub_rn(cur, corr), 0.0f);
+}
+
+}  // namespace ldpcb200

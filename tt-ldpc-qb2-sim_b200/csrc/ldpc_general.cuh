@@ -1,0 +1,58 @@
+// Decoder for an arbitrary parity-check matrix with the reference's serial row order.
+//
+// The reference updates rows one after another in file order (engines/scalar_5w/ldpc_decoder_core.h:
+// 314-522).  The host splits that order into runs of consecutive rows that share no variable; rows of
+// one run are independent, so updating them at once gives the serial result bit for bit.  One warp
+// owns one frame: lanes take the rows of a run (32 at a time), __syncwarp between runs.  L lives in
+// shared memory; the messages r of a slot live in a global-memory scratch area laid out [edge][row] so
+// a warp's accesses to one edge of 32 consecutive rows coalesce (the area of all resident slots,
+// E x 2-4 bytes each, stays in L2).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/ldpcb200.h"
+#include "ldpc_device.cuh"
+
+namespace ldpcb200 {
+
+constexpr int GEN_WARPS = 4;  // frame slots (warps) per CTA
+
+struct GeneralCode {
+    int N = 0, M = 0, P = 0, dmax = 0, n_runs = 0, dt = 0;  // dt: compiled degree bound
+    int32_t* d_cols = nullptr;  // [dmax][M] column of edge e of row m (-1 pad)
+    int32_t* d_runs = nullptr;  // [n_runs + 1] first row of each run, then M
+    void* d_r = nullptr;        // message scratch: [slots][dmax][M] elements
+    size_t r_cap = 0;
+};
+
+struct GenParams {
+    const int32_t* cols;
+    const int32_t* runs;
+    int32_t n_runs, N, M, n_tx, dmax, max_iter;
+    float mu, sigma, l_max, r_max, l_post_max;
+    uint32_t seed_lo, seed_hi, stream;
+    uint64_t first_frame;
+    uint32_t n_frames;
+    void* r_base;
+    const float* llr_in;
+    float* post_out;
+    int32_t* iters_out;
+    int32_t* synd_out;
+    int32_t* be_out;
+    unsigned long long* tally;
+    unsigned long long* hist;
+    int32_t hist_bins;
+    unsigned int* work;
+};
+
+int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCode* g, std::string& err);
+void free_general(GeneralCode* g);
+int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
+                   const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
+                   unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,
+                   int n_sm, cudaStream_t stream, std::string& err);
+
+}  // namespace ldpcb200

@@ -1,0 +1,420 @@
+// Layered decoder for quasi-cyclic AR4JA codes on sm_100a: channel generation, row-layered
+// Approximate-Min* (or normalised min-sum) decoding with syndrome stop, and error tallies, in one
+// persistent kernel.
+//
+// Code structure (see ldpcb200/ar4ja.py): 12 layers of Z rows; layers 0-3 have degree 3, layers 4-11
+// degree D; row j of layer l checks columns blk_off[l][e] + ((j + shift[l][e]) mod Z) for its edges e
+// in ascending column order.  Rows inside a layer share no column, so the Z rows of a layer are
+// updated at once and the result equals the reference's serial row loop
+// (engines/scalar_5w/ldpc_decoder_core.h:311-522) bit for bit.
+//
+// Mapping.  One CTA of T = Z/R threads owns F frame slots.  Thread t updates rows t, t+T, ... of
+// every layer (R rows), for all F slots in lockstep:
+//   * L (posterior LLRs, N per slot) lives in shared memory: bf16 in the reference-numerics mode,
+//     fp32 otherwise;
+//   * the check-to-variable messages r of the thread's own rows never leave registers: 12 layers x R
+//     rows x F slots x degree values, as packed 16-bit pairs (bf16 / fp16 storage) or fp32;
+//   * the circulant shift is the address rotation (j + shift) & (Z-1) into the shared L array;
+//   * after each iteration from the third on, hard decisions are packed with warp ballots and the
+//     syndrome of each 32-row word is the XOR of the edge blocks' bit vectors rotated by their shifts
+//     (funnel shifts), i.e. 12*Z/32 words per frame instead of one parity per row.
+// A slot whose frame converges (or reaches max_iter) is tallied and refilled at once from a global
+// frame counter: early-retire with slot refill, so fast and slow frames never wait for each other.
+#pragma once
+#include <cstdint>
+#include "ldpc_device.cuh"
+
+namespace ldpcb200 {
+
+constexpr int QC_LAYERS = 12;
+constexpr int QC_DEG_LOW = 3;  // degree of layers 0-3 (block row 0 of every AR4JA code)
+constexpr int QC_DMAX = 18;
+constexpr int QC_MAX_F = 4;
+
+// Kernel arguments (one copy in the constant parameter bank; every descriptor read is a constant
+// operand, not a memory instruction).
+struct QcParams {
+    int32_t blk_off[QC_LAYERS][QC_DMAX];  // column block * Z of edge e of layer l
+    int32_t shift[QC_LAYERS][QC_DMAX];    // circulant shift of edge e of layer l
+    int32_t n_vars;                       // N
+    int32_t n_tx;                         // N - P: the transmitted prefix
+    int32_t max_iter;
+    float mu, sigma;                      // channel LLR mean and standard deviation
+    float l_max, r_max, l_post_max;       // clips (0 = off)
+    uint32_t seed_lo, seed_hi, stream;
+    uint64_t first_frame;                 // global index of this launch's frame 0
+    uint32_t n_frames;
+    const float* llr_in;                  // external channel LLRs [n_frames][n_tx] (or null)
+    float* post_out;                      // [n_frames][N] posteriors (optional)
+    int32_t* iters_out;                   // [n_frames] (optional)
+    int32_t* synd_out;                    // [n_frames] failing rows after decoding (optional)
+    int32_t* be_out;                      // [n_frames] bit errors (optional)
+    unsigned long long* tally;            // [TALLY_WORDS]
+    unsigned long long* hist;             // [hist_bins] iterations histogram (optional)
+    int32_t hist_bins;
+    unsigned int* work;                   // frame claim counter, zero at launch
+};
+
+enum TallyWord : int {
+    T_FRAMES = 0, T_BIT_ERR, T_FRAME_ERR, T_ITER_SUM, T_UNCONVERGED, T_MAX_ITER, T_CYCLES, TALLY_WORDS = 8
+};
+
+template <int MODE> struct LTraits;
+template <> struct LTraits<STORE_BF16> {
+    using T = uint16_t;
+    static __device__ __forceinline__ float ld(const T* s, int i) { return __uint_as_float(uint32_t(s[i]) << 16); }
+    static __device__ __forceinline__ void st(T* s, int i, float v) { s[i] = __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+    static __device__ __forceinline__ uint32_t sign(const T* s, int i) { return uint32_t(s[i]) >> 15; }
+    static __device__ __forceinline__ float round_ch(float v) { return bf16_round(v); }
+};
+template <> struct LTraits<STORE_FP32> {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T* s, int i) { return s[i]; }
+    static __device__ __forceinline__ void st(T* s, int i, float v) { s[i] = v; }
+    static __device__ __forceinline__ uint32_t sign(const T* s, int i) { return __float_as_uint(s[i]) >> 31; }
+    static __device__ __forceinline__ float round_ch(float v) { return v; }
+};
+template <> struct LTraits<STORE_FP16> : LTraits<STORE_FP32> {};
+
+// Messages of one row in registers.
+template <int d, int MODE> struct RowMsg {  // 16-bit storage: pairs packed in 32-bit words
+    uint32_t w[(d + 1) / 2];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < (d + 1) / 2; ++i) w[i] = 0u;
+    }
+    __device__ __forceinline__ float get(int e) const {
+        const uint32_t x = w[e >> 1];
+        if (MODE == STORE_BF16) return (e & 1) ? __uint_as_float(x & 0xFFFF0000u) : __uint_as_float(x << 16);
+        const __half2 h = *reinterpret_cast<const __half2*>(&x);
+        return (e & 1) ? __high2float(h) : __low2float(h);
+    }
+    __device__ __forceinline__ void set2(int e, float a, float b) {  // e even: edges e and e+1
+        uint32_t x;
+        if (MODE == STORE_BF16) {
+            __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+            x = *reinterpret_cast<uint32_t*>(&v);
+        } else {
+            a = fminf(fmaxf(a, -65504.0f), 65504.0f);
+            b = fminf(fmaxf(b, -65504.0f), 65504.0f);
+            __half2 v = __floats2half2_rn(a, b);
+            x = *reinterpret_cast<uint32_t*>(&v);
+        }
+        w[e >> 1] = x;
+    }
+};
+template <int d> struct RowMsg<d, STORE_FP32> {
+    float v[d];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < d; ++i) v[i] = 0.0f;
+    }
+    __device__ __forceinline__ float get(int e) const { return v[e]; }
+    __device__ __forceinline__ void set2(int e, float a, float b) {
+        v[e] = a;
+        if (e + 1 < d) v[e + 1] = b;
+    }
+};
+
+// Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
+// sL + f*lstride).  idx[e]: the row's column indices.
+template <int d, int MODE, int ALGO, bool CLIP, int F>
+__device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
+                                           RowMsg<d, MODE> (&rm)[F], float r_cap, float lp_cap) {
+    using LT = LTraits<MODE>;
+    float q[F][d];
+#pragma unroll
+    for (int f = 0; f < F; ++f)
+#pragma unroll
+        for (int e = 0; e < d; ++e) q[f][e] = __fsub_rn(LT::ld(sL + f * lstride, idx[e]), rm[f].get(e));
+
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+        uint32_t par = 0;
+#pragma unroll
+        for (int e = 0; e < d; ++e) par ^= __float_as_uint(q[f][e]);
+        par &= 0x80000000u;
+        int am = 0;
+        float mag_min, mag_all;
+        if (ALGO == ALGO_AMIN) {
+            // argmin of |q| with a strict < from 9999 (first minimum wins), then the recursive min*
+            // over the other edges in row order and a final step with the minimum
+            // (ldpc_decoder_core.h:414-475, 176-201).
+            float mn = 9999.0f;
+#pragma unroll
+            for (int e = 0; e < d; ++e) {
+                const float a = fabsf(q[f][e]);
+                const bool lt = a < mn;
+                mn = lt ? a : mn;
+                am = lt ? e : am;
+            }
+            float m = __int_as_float(0x7f800000);
+#pragma unroll
+            for (int e = 0; e < d; ++e) {
+                const float nm = amin_step(m, fabsf(q[f][e]));
+                m = (e == am) ? m : nm;
+            }
+            mag_min = m;
+            mag_all = amin_step(m, mn);
+        } else {
+            // normalised min-sum, alpha = 0.75 (ldpc_decoder_core.h:322-379)
+            float m1 = 999.0f, m2 = 999.0f;
+#pragma unroll
+            for (int e = 0; e < d; ++e) {
+                const float a = fabsf(q[f][e]);
+                const bool l1 = a < m1, l2 = a < m2;
+                m2 = l1 ? m1 : (l2 ? a : m2);
+                am = l1 ? e : am;
+                m1 = l1 ? a : m1;
+            }
+            mag_min = __fmul_rn(0.75f, m2);
+            mag_all = __fmul_rn(0.75f, m1);
+        }
+        if (CLIP) {
+            mag_min = fminf(mag_min, r_cap);
+            mag_all = fminf(mag_all, r_cap);
+        }
+        // r_e = +-mag with sign parity ^ sign(q_e): fold the parity into the magnitudes once.
+        const uint32_t smin = __float_as_uint(mag_min) | par;
+        const uint32_t sall = __float_as_uint(mag_all) | par;
+        float rn[d];
+#pragma unroll
+        for (int e = 0; e < d; ++e) {
+            const uint32_t sel = (e == am) ? smin : sall;
+            rn[e] = __uint_as_float(sel ^ (__float_as_uint(q[f][e]) & 0x80000000u));
+            float ln = __fadd_rn(q[f][e], rn[e]);
+            if (CLIP) ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
+            LT::st(sL + f * lstride, idx[e], ln);
+        }
+#pragma unroll
+        for (int e = 0; e < d; e += 2) rm[f].set2(e, rn[e], (e + 1 < d) ? rn[e + 1] : 0.0f);
+    }
+}
+
+template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT>
+__global__ void __launch_bounds__(Z / R) qc_decode_kernel(const __grid_constant__ QcParams p) {
+    constexpr int T = Z / R;
+    constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
+    static_assert(Z % 32 == 0 && Z % R == 0 && T % 32 == 0, "Z must be a multiple of 32 and of 32*R");
+    static_assert(F >= 1 && F <= QC_MAX_F, "frames per CTA");
+    using LT = LTraits<MODE>;
+    using LE = typename LT::T;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N = p.n_vars;
+    const int nblk = N / Z;
+    const int lstride = (N + 7) & ~7;                      // elements per slot (16-byte multiple)
+    LE* sL = reinterpret_cast<LE*>(smem_raw);
+    uint32_t* sHB = reinterpret_cast<uint32_t*>(smem_raw + (size_t)F * lstride * sizeof(LE));  // [F][nblk*W]
+    __shared__ uint32_t s_fid[QC_MAX_F];
+    __shared__ uint32_t s_fail;
+    __shared__ uint32_t s_sfail[QC_MAX_F];
+    __shared__ uint32_t s_be[QC_MAX_F];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
+    const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
+
+    RowMsg<QC_DEG_LOW, MODE> r3[4][R][F];
+    RowMsg<D, MODE> rD[8][R][F];
+
+    uint32_t act = 0;                // active slots (uniform)
+    uint32_t need = (1u << F) - 1u;  // slots waiting for a frame (uniform)
+    int it[F];
+    uint32_t fid[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) { it[f] = 0; fid[f] = 0xFFFFFFFFu; }
+
+    // per-CTA tallies, kept by thread 0
+    unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0;
+
+    for (;;) {
+        // ---------------------------------------------------------------- refill
+        if (need) {
+            if (tid == 0) {
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+                    if (need & (1u << f)) {
+                        const uint32_t c = atomicAdd(p.work, 1u);
+                        s_fid[f] = c < p.n_frames ? c : 0xFFFFFFFFu;
+                    }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int f = 0; f < F; ++f) {
+                if (!(need & (1u << f))) continue;
+                fid[f] = s_fid[f];
+                it[f] = 0;
+                if (fid[f] == 0xFFFFFFFFu) { act &= ~(1u << f); continue; }
+                act |= 1u << f;
+#pragma unroll
+                for (int l = 0; l < 4; ++l)
+#pragma unroll
+                    for (int rho = 0; rho < R; ++rho) r3[l][rho][f].zero();
+#pragma unroll
+                for (int l = 0; l < 8; ++l)
+#pragma unroll
+                    for (int rho = 0; rho < R; ++rho) rD[l][rho][f].zero();
+                LE* L = sL + f * lstride;
+                const int nq = p.n_tx >> 2;
+                if (EXT) {
+                    const float4* src = reinterpret_cast<const float4*>(p.llr_in + (size_t)fid[f] * p.n_tx);
+                    for (int qd = tid; qd < nq; qd += T) {
+                        const float4 v4 = src[qd];
+                        float v[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            float x = v[k];
+                            if (CLIP && p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
+                            LT::st(L, 4 * qd + k, x);
+                        }
+                    }
+                } else {
+                    const uint64_t gf = p.first_frame + fid[f];
+                    for (int qd = tid; qd < nq; qd += T) {
+                        float n[4];
+                        if (p.sigma > 0.0f) {
+                            const U32x4 x = philox4x32_10(U32x4{(uint32_t)qd, (uint32_t)gf, (uint32_t)(gf >> 32), p.stream},
+                                                          p.seed_lo, p.seed_hi);
+                            box_muller(x.x, x.y, n[0], n[1]);
+                            box_muller(x.z, x.w, n[2], n[3]);
+                        } else {
+                            n[0] = n[1] = n[2] = n[3] = 0.0f;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            float x = p.sigma > 0.0f ? __fmaf_rn(p.sigma, n[k], p.mu) : p.mu;
+                            if (CLIP && p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
+                            LT::st(L, 4 * qd + k, x);
+                        }
+                    }
+                }
+                for (int i = p.n_tx + tid; i < N; i += T) LT::st(L, i, 0.0f);
+            }
+            need = 0;
+            __syncthreads();
+        }
+        if (!act) break;
+
+        // ---------------------------------------------------------------- one layered iteration
+        if (p.max_iter > 0) {
+#pragma unroll
+            for (int l = 0; l < QC_LAYERS; ++l) {
+#pragma unroll
+                for (int rho = 0; rho < R; ++rho) {
+                    const int j = tid + rho * T;
+                    if (l < 4) {
+                        int idx[QC_DEG_LOW];
+#pragma unroll
+                        for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                        row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, r3[l & 3][rho], r_cap, lp_cap);
+                    } else {
+                        int idx[D];
+#pragma unroll
+                        for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                        row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rD[(l - 4) & 7][rho], r_cap, lp_cap);
+                    }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int f = 0; f < F; ++f) it[f] += (act >> f) & 1u;
+        }
+
+        // ---------------------------------------------------------------- syndrome / stop
+        uint32_t eval = 0;
+#pragma unroll
+        for (int f = 0; f < F; ++f)
+            if ((act >> f) & 1u)
+                if (it[f] >= 3 || it[f] >= p.max_iter) eval |= 1u << f;
+        if (!eval) continue;
+
+        const int nwords = nblk * W;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            if (!((eval >> f) & 1u)) continue;
+            const LE* L = sL + f * lstride;
+            uint32_t* hb = sHB + f * nwords;
+            for (int wd = warp; wd < nwords; wd += T / 32) {
+                const uint32_t b = __ballot_sync(0xFFFFFFFFu, LT::sign(L, wd * 32 + lane));
+                if (lane == 0) hb[wd] = b;
+            }
+        }
+        if (tid < F) { s_sfail[tid] = 0; s_be[tid] = 0; }
+        __syncthreads();
+        // syndrome words: (f, layer, word) -> XOR over the layer's edges of the rotated block vectors
+        for (int t = tid; t < F * QC_LAYERS * W; t += T) {
+            const int f = t / (QC_LAYERS * W);
+            if (!((eval >> f) & 1u)) continue;
+            const int l = (t / W) % QC_LAYERS, w = t % W;
+            const uint32_t* hb = sHB + f * nwords;
+            const int deg = l < 4 ? QC_DEG_LOW : D;
+            uint32_t acc = 0;
+            for (int e = 0; e < deg; ++e) {
+                const int s = p.shift[l][e];
+                const int base = p.blk_off[l][e] >> 5;
+                const int ws = s >> 5;
+                const uint32_t lo = hb[base + ((w + ws) & (W - 1))];
+                const uint32_t hi = hb[base + ((w + ws + 1) & (W - 1))];
+                acc ^= __funnelshift_r(lo, hi, s & 31);
+            }
+            if (acc) atomicAdd(&s_sfail[f], (uint32_t)__popc(acc));
+        }
+        // bit errors over the transmitted prefix
+        const int ntxw = p.n_tx >> 5;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            if (!((eval >> f) & 1u)) continue;
+            const uint32_t* hb = sHB + f * nwords;
+            uint32_t cnt = 0;
+            for (int t = tid; t < ntxw; t += T) cnt += __popc(hb[t]);
+            cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+            if (lane == 0 && cnt) atomicAdd(&s_be[f], cnt);
+        }
+        __syncthreads();
+        uint32_t done = 0;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            if (!((eval >> f) & 1u)) continue;
+            const bool conv = it[f] >= 3 && s_sfail[f] == 0;
+            if (conv || it[f] >= p.max_iter) done |= 1u << f;
+        }
+        if (!done) continue;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+            if (!((done >> f) & 1u)) continue;
+            const uint32_t be = s_be[f], sf = s_sfail[f];
+            if (tid == 0) {
+                t_frames += 1;
+                t_be += be;
+                t_fe += be > 0;
+                t_it += (unsigned)it[f];
+                t_unc += sf != 0;
+                t_max = max(t_max, (unsigned long long)it[f]);
+                if (p.hist) atomicAdd(&p.hist[min(it[f], p.hist_bins - 1)], 1ull);
+                if (p.iters_out) p.iters_out[fid[f]] = it[f];
+                if (p.synd_out) p.synd_out[fid[f]] = (int32_t)sf;
+                if (p.be_out) p.be_out[fid[f]] = (int32_t)be;
+            }
+            if (p.post_out) {
+                const LE* L = sL + f * lstride;
+                float* dst = p.post_out + (size_t)fid[f] * N;
+                for (int i = tid; i < N; i += T) dst[i] = LT::ld(L, i);
+            }
+        }
+        need = done;
+        act &= ~done;
+        __syncthreads();  // s_be / s_sfail / sL of finished slots are reused below
+    }
+    if (tid == 0 && t_frames) {
+        atomicAdd(&p.tally[T_FRAMES], t_frames);
+        atomicAdd(&p.tally[T_BIT_ERR], t_be);
+        atomicAdd(&p.tally[T_FRAME_ERR], t_fe);
+        atomicAdd(&p.tally[T_ITER_SUM], t_it);
+        atomicAdd(&p.tally[T_UNCONVERGED], t_unc);
+        atomicMax(&p.tally[T_MAX_ITER], t_max);
+    }
+}
+
+}  // namespace ldpcb200

@@ -1,0 +1,46 @@
+// Registry of compiled kernel variants.  Each instantiation unit (qc_inst_*.cu, general.cu) adds its
+// kernels to a table the host API searches by shape; a shape that was not built is reported as
+// LDPC_ENOTSUP instead of being emulated.
+#pragma once
+#include <cstdint>
+
+namespace ldpcb200 {
+
+struct QcKey {
+    int Z, D, R, F, mode, algo, clip, ext;
+    bool operator==(const QcKey& o) const {
+        return Z == o.Z && D == o.D && R == o.R && F == o.F && mode == o.mode && algo == o.algo &&
+               clip == o.clip && ext == o.ext;
+    }
+};
+
+struct QcEntry {
+    QcKey key;
+    const void* fn;  // __global__ void (const QcParams)
+};
+
+struct QcTable {
+    const QcEntry* entries;
+    int count;
+    const QcTable* next;
+};
+
+// Linked at static-initialisation time by each instantiation unit.
+void register_qc_table(QcTable* t);
+const QcTable* qc_tables();
+
+}  // namespace ldpcb200
+
+#define LDPC_QC_ENTRY(Z, D, R, F, MODE, ALGO, CLIP, EXT)                       \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT},                                      \
+     reinterpret_cast<const void*>(&::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT>)}
+
+#define LDPC_QC_REGISTER(name)                                                           \
+    namespace {                                                                          \
+    struct name##_reg {                                                                  \
+        name##_reg() {                                                                   \
+            static ::ldpcb200::QcTable t{name, (int)(sizeof(name) / sizeof(name[0])), nullptr}; \
+            ::ldpcb200::register_qc_table(&t);                                           \
+        }                                                                                \
+    } name##_reg_instance;                                                               \
+    }

@@ -1,0 +1,27 @@
+// Kernel variants for Z = 128, D = 6: AR4JA rate 1/2, K = 1024 (N = 2560, 1536 checks).
+#include "ldpc_qc.cuh"
+#include "ldpc_registry.h"
+
+using namespace ldpcb200;
+
+static const QcEntry qc_r12k1[] = {
+    // simulation (Philox channel), Approximate-Min*, no clips: the benchmarked path
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 2, STORE_BF16, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP32, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP16, ALGO_AMIN, false, false),
+    // caller-supplied LLRs (parity tests, ldpc_decode_llr)
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, true),
+    // reference-engine options: -n (NMS) and the -L/-R/-V/-G clips, reference numerics
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, true, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, true, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, true, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, false, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, true, true),
+};
+LDPC_QC_REGISTER(qc_r12k1)

@@ -1,0 +1,219 @@
+"""ctypes binding of libldpcb200 (include/ldpcb200.h).
+
+There is no CPU path behind this module: if the library is missing, or no sm_100 GPU is present,
+every call raises.  ``Decoder`` owns one handle (one CUDA stream); use it from one thread at a time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libldpcb200.so")
+
+STORE_BF16, STORE_FP32, STORE_FP16 = 0, 1, 2
+ALGO_AMIN, ALGO_NMS = 0, 1
+KERNEL_QC, KERNEL_GENERAL = 0, 1
+STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
+
+# The entry points include/ldpcb200.h declares (tests check that the library exports each one).
+EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
+           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_launch_count",
+           "ldpc_last_error", "ldpc_abi_version")
+
+
+class LdpcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+class LibraryMissing(LdpcError):
+    pass
+
+
+class Matrix(C.Structure):
+    _fields_ = [("n_vars", C.c_int32), ("n_checks", C.c_int32), ("n_punct", C.c_int32),
+                ("max_check_deg", C.c_int32), ("rows", C.POINTER(C.c_int32))]
+
+
+class RunParams(C.Structure):
+    _fields_ = [("mu", C.c_float), ("sigma", C.c_float), ("seed", C.c_uint64), ("stream", C.c_uint32),
+                ("reserved0", C.c_uint32), ("first_frame", C.c_uint64), ("n_frames", C.c_uint64),
+                ("max_iter", C.c_int32), ("storage", C.c_int32), ("algo", C.c_int32),
+                ("l_max", C.c_float), ("r_max", C.c_float), ("l_post_max", C.c_float)]
+
+
+class Tally(C.Structure):
+    _fields_ = [("frames", C.c_uint64), ("bit_errors", C.c_uint64), ("frame_errors", C.c_uint64),
+                ("iter_sum", C.c_uint64), ("unconverged", C.c_uint64), ("max_iters", C.c_uint64),
+                ("kernel_ms", C.c_float), ("reserved1", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (once).  Raises LibraryMissing if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise LibraryMissing(-2, f"{path} is missing: build it with `python -m ldpcb200.build` "
+                                 "(or __graft_entry__.build()); there is no CPU fallback")
+    L = C.CDLL(path)
+    P = C.POINTER
+    L.ldpc_create.argtypes = [P(Matrix), C.c_int, P(C.c_void_p)]
+    L.ldpc_destroy.argtypes = [C.c_void_p]
+    L.ldpc_destroy.restype = None
+    L.ldpc_kernel_kind.argtypes = [C.c_void_p]
+    L.ldpc_run_chunk.argtypes = [C.c_void_p, P(RunParams), P(Tally)]
+    L.ldpc_decode_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), C.c_int64, P(C.c_float),
+                                  P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
+    L.ldpc_channel_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float)]
+    L.ldpc_iter_histogram.argtypes = [C.c_void_p, P(C.c_uint64), C.c_int]
+    L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.ldpc_launch_count.argtypes = [C.c_void_p]
+    L.ldpc_launch_count.restype = C.c_int64
+    L.ldpc_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.ldpc_abi_version.argtypes = []
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load().ldpc_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc: int):
+    if rc < 0:
+        raise LdpcError(rc, last_error())
+    return rc
+
+
+def channel_mu_sigma(N: int, M: int, P: int, ebn0_db: float):
+    """mu = 4 R Eb/N0, sigma = sqrt(8 R Eb/N0) with R = (N-M)/(N-P), computed in double and rounded to
+    float (engines/scalar_5w/ldpc_sim_scalar.cpp:351-355)."""
+    rate = (N - M) / (N - P)
+    snr = 10.0 ** (ebn0_db / 10.0)
+    return float(np.float32(4.0 * rate * snr)), float(np.float32(math.sqrt(8.0 * rate * snr)))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32)) if a is not None else None
+
+
+@dataclass
+class ChunkResult:
+    frames: int
+    bit_errors: int
+    frame_errors: int
+    iter_sum: int
+    unconverged: int
+    max_iters: int
+    kernel_ms: float
+
+
+class Decoder:
+    """One parity-check matrix on one GPU.  ``rows``: [M, dmax] int32, 0-based columns in file order,
+    -1 padded; the last ``n_punct`` of the ``n_vars`` columns are punctured."""
+
+    def __init__(self, rows: np.ndarray, n_vars: int, n_punct: int, device: int = -1):
+        self._lib = load()
+        self.rows = np.ascontiguousarray(rows, dtype=np.int32)
+        self.M, self.dmax = self.rows.shape
+        self.N, self.P = int(n_vars), int(n_punct)
+        self.n_tx = self.N - self.P
+        m = Matrix(self.N, self.M, self.P, self.dmax, _ip(self.rows))
+        h = C.c_void_p()
+        _check(self._lib.ldpc_create(C.byref(m), device, C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_code(cls, code, device: int = -1) -> "Decoder":
+        """From an ``ar4ja.QcCode`` (makeH order) or a ``chinn.Matrix`` plus punctured count."""
+        return cls(code.row_matrix(), code.N, code.P, device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ldpc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def kind(self) -> int:
+        return _check(self._lib.ldpc_kernel_kind(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.ldpc_launch_count(self._h))
+
+    def set_launch_shape(self, rows_per_thread: int = 0, frames_per_cta: int = 0):
+        _check(self._lib.ldpc_set_launch_shape(self._h, rows_per_thread, frames_per_cta))
+
+    @staticmethod
+    def params(mu=0.0, sigma=0.0, seed=1, stream=0, first_frame=0, n_frames=0, max_iter=200,
+               storage=STORE_BF16, algo=ALGO_AMIN, l_max=0.0, r_max=0.0, l_post_max=0.0) -> RunParams:
+        if isinstance(storage, str):
+            storage = STORAGE_NAMES[storage]
+        return RunParams(mu, sigma, seed, stream, 0, first_frame, n_frames, max_iter, storage, algo,
+                         l_max, r_max, l_post_max)
+
+    def run_chunk(self, p: RunParams) -> ChunkResult:
+        t = Tally()
+        _check(self._lib.ldpc_run_chunk(self._h, C.byref(p), C.byref(t)))
+        return ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged,
+                           t.max_iters, t.kernel_ms)
+
+    def decode_llr(self, llr: np.ndarray, p: Optional[RunParams] = None, want_post: bool = True, **kw):
+        """Decode caller-supplied channel LLRs [n, N-P].  Returns (post [n, N] or None, iters,
+        synd_fail, bit_errors, ChunkResult)."""
+        if p is None:
+            p = self.params(**kw)
+        llr = np.ascontiguousarray(np.atleast_2d(llr), dtype=np.float32)
+        if llr.shape[1] != self.n_tx:
+            raise ValueError(f"llr has {llr.shape[1]} columns, expected N-P = {self.n_tx}")
+        n = llr.shape[0]
+        post = np.empty((n, self.N), np.float32) if want_post else None
+        it = np.empty(n, np.int32)
+        sf = np.empty(n, np.int32)
+        be = np.empty(n, np.int32)
+        t = Tally()
+        _check(self._lib.ldpc_decode_llr(self._h, C.byref(p), _fp(llr), n, _fp(post), _ip(it), _ip(sf),
+                                         _ip(be), C.byref(t)))
+        return post, it, sf, be, ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum,
+                                             t.unconverged, t.max_iters, t.kernel_ms)
+
+    def channel_llr(self, p: RunParams) -> np.ndarray:
+        out = np.empty((int(p.n_frames), self.n_tx), np.float32)
+        _check(self._lib.ldpc_channel_llr(self._h, C.byref(p), _fp(out)))
+        return out
+
+    def iter_histogram(self, n_bins: int = 256) -> np.ndarray:
+        h = np.zeros(n_bins, np.uint64)
+        _check(self._lib.ldpc_iter_histogram(self._h, h.ctypes.data_as(C.POINTER(C.c_uint64)), n_bins))
+        return h
