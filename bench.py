@@ -1,0 +1,433 @@
+#!/usr/bin/env python3
+"""Benchmark of the AR4JA Monte Carlo hot path on B200.
+
+Workload (the error-floor configuration of the rate-1/2 K=1024 code): AR4JA rate 1/2, K = 1024,
+N = 2560 (512 punctured columns, 2048 transmitted symbols), all-zero codeword, BPSK over AWGN,
+Eb/N0 = 2.5 dB and 3.0 dB, layered Approximate-Min* with at most 200 iterations and the syndrome
+stop, per-frame Philox-4x32-10 counters (seed 1, frame index).  One step = ``--frames`` frames per
+Eb/N0 point per GPU: channel generation, decoding and error tallies, all inside the fused kernel.
+
+Metric: channel symbols per second (Gsps; frames/s reported beside it).  ``value`` is device time
+(CUDA events around each decode launch on the library's stream) over K steps, max over ranks;
+``e2e`` is the same work timed around each call of the C ABI (``ldpc_run_chunk``: parameters from
+the host, tallies back to the host).  The reference arm (``--impl reference``) times the
+reference's own CPU decoder (run_ldpc_worker, built from its sources into oracle/_ref) on every
+host thread on the same workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "tt-ldpc-qb2-sim_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "channel Gsps & frames/s at 200 iter (1 B200) vs CPU golden; FER-matched speedup"
+UNIT = "Gsps"
+POINTS = (2.5, 3.0)
+MAX_ITER = 200
+SEED = 1
+LANE_OPS_PER_EDGE = 20        # algorithmic lane operations per edge per executed iteration
+BYTES_PER_EDGE = {"fp32": 16, "fp16": 12, "bf16": 8}  # read+write of L and r per edge update
+SM_COUNT = 148
+LANES_PER_SM = 128
+SMEM_BYTES_PER_CLK = 128
+PROFILE_SUMMARY = os.path.join(REPO, "profiles", "qc_decode_r12k1_fp32_ncu.txt")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--frames", type=int, default=1 << 22, help="frames per Eb/N0 point per GPU per step")
+    ap.add_argument("--storage", choices=("fp32", "fp16", "bf16"), default="fp32")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the other storage modes")
+    ap.add_argument("--ref-step-seconds", type=float, default=2.0,
+                    help="reference arm: CPU seconds per Eb/N0 point per step")
+    return ap.parse_args()
+
+
+def code_and_matrix():
+    from ldpcb200 import ar4ja
+    return ar4ja.make_code(1024, "1/2")
+
+
+def mu_sigma(code, ebn0):
+    from ldpcb200.capi import channel_mu_sigma
+    return channel_mu_sigma(code.N, code.n_checks, code.P, ebn0)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpus):
+        self.gpus = gpus
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ",".join(str(g) for g in self.gpus), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(seconds: float, threads: int = 0):
+    """The reference's own decoder (oracle/_ref/ref_mc) on every host thread, else the oracle port."""
+    from oracle import oracle as O
+    code = code_and_matrix()
+    oc = O.Code(code.row_matrix(), code.N, code.P)
+    threads = threads or os.cpu_count() or 1
+    per_point = max(1.0, seconds / len(POINTS))
+    frames = fe = be = 0
+    el = 0.0
+    it0 = n0 = 0
+    kind = "reference" if O.ref_binary("ref_mc") else "port"
+    for eb in POINTS:
+        mu, sigma = mu_sigma(code, eb)
+        if kind == "reference":
+            r = O.run_ref_mc(oc, mu, sigma, MAX_ITER, 1 << 40, per_point, seed=SEED, threads=threads)
+            frames += r["frames"]; fe += r["frame_errors"]; be += r["bit_errors"]
+            el += r["elapsed_s"]; it0 += r["cw0_iter_sum"]; n0 += r["cw0_count"]
+        else:
+            r = _port_mc(oc, mu, sigma, per_point, threads)
+            frames += r[0]; be += r[1]; fe += r[2]; it0 += r[3]; n0 += r[0]; el += r[4]
+    fps = frames / el if el > 0 else 0.0
+    return {
+        "value": round(fps * code.n_tx / 1e9, 6), "unit": UNIT, "cores": threads, "kind": kind,
+        "frames_per_s": round(fps, 1),
+        "sample": (f"{frames} frames over {el:.1f} s: Eb/N0 {POINTS[0]} and {POINTS[1]} dB, "
+                   f"{per_point:.0f} s each, max {MAX_ITER} iterations, bf16 reference numerics, "
+                   f"xoshiro128+/polar channel; mean iterations {it0 / max(n0, 1):.2f}, FER {fe / max(frames, 1):.2e}"),
+    }
+
+
+def _port_mc(oc, mu, sigma, seconds, threads):
+    """Threaded oracle Monte Carlo (the restatement, run in C; ctypes drops the GIL)."""
+    import numpy as np
+    from oracle import oracle as O
+    stop = time.perf_counter() + seconds
+    out = [[0, 0, 0, 0] for _ in range(threads)]
+
+    def work(t):
+        s = O.xo_seed(1000 + t)
+        while time.perf_counter() < stop:
+            tal = O.mc_pairs(oc, MAX_ITER, mu, sigma, s, 4)
+            for k in range(4):
+                out[t][k] += int(tal[k])
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    el = time.perf_counter() - t0
+    tot = np.array(out).sum(0)
+    return int(tot[0]), int(tot[1]), int(tot[2]), int(tot[3]), el
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    code = code_and_matrix()
+    oc = O.Code(code.row_matrix(), code.N, code.P)
+    threads = os.cpu_count() or 1
+    kind = "reference" if O.ref_binary("ref_mc") else "port"
+    frames = fe = 0
+    el = 0.0
+    for step in range(args.warmup + args.steps):
+        for eb in POINTS:
+            mu, sigma = mu_sigma(code, eb)
+            if kind == "reference":
+                r = O.run_ref_mc(oc, mu, sigma, MAX_ITER, 1 << 40, args.ref_step_seconds, seed=SEED + step,
+                                 threads=threads)
+                f, e, t = r["frames"], r["frame_errors"], r["elapsed_s"]
+            else:
+                f, _, e, _, t = _port_mc(oc, mu, sigma, args.ref_step_seconds, threads)
+            if step >= args.warmup:
+                frames += f; fe += e; el += t
+    value = frames * code.n_tx / el / 1e9 if el > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * el / max(args.steps, 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: all-zero codeword, BPSK over AWGN, the reference's xoshiro128+/polar channel",
+        "impl": "reference",
+        "config": {"workload": "AR4JA r1/2 K=1024 N=2560, Eb/N0 2.5 and 3.0 dB, max 200 iterations, syndrome stop",
+                   "engine": "run_ldpc_worker (engines/scalar_5w/ldpc_decoder_core.h) on host threads",
+                   "frames_per_s": round(frames / el, 1) if el > 0 else 0.0, "fer": fe / max(frames, 1)},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{frames} frames over {el:.1f} s in {args.steps} steps of "
+                                   f"{args.ref_step_seconds:.1f} s per Eb/N0 point"},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def profile_traffic():
+    """DRAM bytes per decode launch from the committed ncu summary (line 'dram_bytes_per_launch: X')."""
+    try:
+        with open(PROFILE_SUMMARY) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def run_ours(args):
+    import torch
+
+    from ldpcb200 import capi
+    from ldpcb200.dist import frame_range
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world and world > 1:
+        log(f"--gpus {args.gpus} but WORLD_SIZE {world}: using WORLD_SIZE")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allreduce(vals, op):
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=op)
+        return t.tolist()
+
+    code = code_and_matrix()
+    dec = capi.Decoder.from_code(code, local)
+    assert dec.kind == capi.KERNEL_QC
+    F = args.frames
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step(i, storage, acc=None):
+        for pi, eb in enumerate(POINTS):
+            mu, sigma = mu_sigma(code, eb)
+            first, _ = frame_range(i, world, rank, F)  # disjoint frame ranges over ranks and steps
+            p = dec.params(mu=mu, sigma=sigma, seed=SEED, stream=pi, first_frame=first, n_frames=F,
+                           max_iter=MAX_ITER, storage=storage)
+            t0 = time.perf_counter()
+            r = dec.run_chunk(p)
+            t1 = time.perf_counter()
+            if acc is not None:
+                a = acc[eb]
+                a["frames"] += r.frames; a["fe"] += r.frame_errors; a["be"] += r.bit_errors
+                a["iters"] += r.iter_sum; a["kernel_ms"] += r.kernel_ms; a["e2e_s"] += t1 - t0
+                a["launches"] += 1
+        flush.zero_()  # L2 flush between steps (outside every timed call)
+
+    for i in range(args.warmup):
+        step(10_000 + i, args.storage)
+    acc = {eb: dict(frames=0, fe=0, be=0, iters=0, kernel_ms=0.0, e2e_s=0.0, launches=0) for eb in POINTS}
+    launches0 = dec.launches
+    barrier()
+    with ClockSampler(list(range(world)) if rank == 0 else []) as clk:
+        w0 = time.perf_counter()
+        for i in range(args.steps):
+            step(i, args.storage, acc)
+        barrier()
+        wall = time.perf_counter() - w0
+    launches = dec.launches - launches0
+    dev_s = sum(a["kernel_ms"] for a in acc.values()) / 1e3
+    e2e_s = sum(a["e2e_s"] for a in acc.values())
+    frames = sum(a["frames"] for a in acc.values())
+    iters = sum(a["iters"] for a in acc.values())
+    maxes = allreduce([dev_s, e2e_s, wall], torch.distributed.ReduceOp.MAX if dist else None)
+    sums = allreduce([frames, iters, launches] + [acc[eb][k] for eb in POINTS for k in ("frames", "fe", "be", "iters")],
+                     torch.distributed.ReduceOp.SUM if dist else None)
+    dev_max, e2e_max, wall_max = maxes
+    tot_frames, tot_iters, tot_launches = sums[0], sums[1], sums[2]
+    per_point_tot = {eb: dict(zip(("frames", "fe", "be", "iters"), sums[3 + 4 * k:7 + 4 * k])) for k, eb in enumerate(POINTS)}
+
+    # storage comparison (not part of the timed region), rank 0's GPU only
+    compare = {}
+    if not args.no_compare:
+        for st in ("fp32", "fp16", "bf16"):
+            if st == args.storage:
+                continue
+            a2 = {eb: dict(frames=0, fe=0, be=0, iters=0, kernel_ms=0.0, e2e_s=0.0, launches=0) for eb in POINTS}
+            step(20_000, st)
+            for i in range(2):
+                step(30_000 + i, st, a2)
+            f2 = sum(a["frames"] for a in a2.values())
+            ms2 = sum(a["kernel_ms"] for a in a2.values())
+            compare[st] = {"gsps": round(f2 * code.n_tx / (ms2 / 1e3) / 1e9, 3),
+                           "mean_iters": round(sum(a["iters"] for a in a2.values()) / f2, 4),
+                           "steps": 2}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(args.cpu_seconds)
+        except Exception as e:  # a missing baseline must not hide the GPU number
+            log(f"cpu baseline failed: {e}")
+            cpu = None
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        dec.close()
+        return 0
+
+    clocks = clk.summary()
+    gsps = tot_frames * code.n_tx / dev_max / 1e9
+    e2e = tot_frames * code.n_tx / e2e_max / 1e9
+    # roofline: the fused decode kernel is issue-bound on chip (no HBM-resident operands)
+    peaks = measured_peaks()
+    f_mhz = clocks["sm_mhz"] if clocks else peaks.get("sm_max_mhz", 1965.0)
+    n_launch_rank0 = sum(a["launches"] for a in acc.values())
+    edges = code.n_edges
+    ops = LANE_OPS_PER_EDGE * edges * iters            # rank 0's algorithmic work
+    achieved = ops / dev_s / 1e12
+    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
+    smem_bytes = BYTES_PER_EDGE[args.storage] * edges * iters
+    smem_peak = SM_COUNT * SMEM_BYTES_PER_CLK * f_mhz * 1e6 / 1e9
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": round(gsps, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * dev_max / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: all-zero codeword, BPSK over AWGN, Philox-4x32-10 channel generated on chip",
+        "config": {
+            "workload": "AR4JA r1/2 K=1024 N=2560 (2048 tx symbols), layered Approximate-Min*, "
+                        "Eb/N0 2.5 and 3.0 dB, max 200 iterations, syndrome stop",
+            "frames_per_point_per_gpu_per_step": F, "storage": args.storage,
+            "parallelism": f"dp{world} (disjoint Philox frame ranges; tallies all-reduced)",
+            "l2": "flushed between steps (256 MiB write); inputs generated on chip, no HBM operands",
+            "frames_per_s": round(tot_frames / dev_max, 1),
+            "points": {str(eb): {
+                "frames": int(v["frames"]), "frame_errors": int(v["fe"]), "bit_errors": int(v["be"]),
+                "mean_iters": round(v["iters"] / max(v["frames"], 1), 4),
+                "gsps": round(acc[eb]["frames"] * code.n_tx / (acc[eb]["kernel_ms"] / 1e3) / 1e9, 3)}
+                for eb, v in per_point_tot.items()},
+            "storage_comparison": compare,
+            "wall_s": round(wall_max, 3),
+        },
+        "e2e": {"value": round(e2e, 4), "unit": UNIT,
+                "h2d_bytes_per_step": int(len(POINTS) * (dec.launch_param_bytes + 64)),
+                "d2h_bytes_per_step": int(len(POINTS) * 64),
+                "path": "ldpc_run_chunk per Eb/N0 point (host params in, host tallies out)"},
+        "gpu_launches": int(tot_launches),
+        "roofline": {
+            "bound": "issue", "unit": "Tlane-op/s",
+            "achieved": round(achieved, 3), "peak": round(peak, 3), "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "kernel": "qc_decode_kernel<128,6,1,1,%s>" % args.storage,
+            "work": f"{LANE_OPS_PER_EDGE} lane-ops x {edges} edges x executed iterations; "
+                    f"{n_launch_rank0} launches averaging {1e3 * dev_s / max(n_launch_rank0, 1):.2f} ms",
+            "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz "
+                           f"({'median SM clock sampled during the run' if clocks else 'max clock, no samples'})",
+            "smem": {"achieved_gbs": round(smem_bytes / dev_s / 1e9, 1), "peak_gbs": round(smem_peak, 1),
+                     "frac": round(smem_bytes / dev_s / 1e9 / smem_peak, 4),
+                     "bytes_per_edge": BYTES_PER_EDGE[args.storage]},
+            "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
+        },
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    dec.close()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

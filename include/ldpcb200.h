@@ -132,6 +132,10 @@ int ldpc_set_launch_shape(ldpc_handle* h, int rows_per_thread, int frames_per_ct
 /* Number of kernel launches the handle issued since creation (for launch accounting). */
 int64_t ldpc_launch_count(const ldpc_handle* h);
 
+/* Bytes of the kernel argument block one decode launch copies to the device (the only host-to-
+ * device traffic of ldpc_run_chunk besides the launch itself). */
+int64_t ldpc_launch_param_bytes(const ldpc_handle* h);
+
 /* Copies the last error message of the calling thread into buf (NUL-terminated); returns its
  * length. */
 int ldpc_last_error(char* buf, size_t len);

@@ -14,6 +14,11 @@ GOLDEN = os.path.join(REPO, "tests", "golden", "golden_scalar_worker.npz")
 REFERENCE = os.environ.get("LDPC_REFERENCE_TREE", "/root/reference")
 
 
+def n_golden_cases() -> int:
+    with np.load(GOLDEN) as d:
+        return sum(1 for k in d.files if k.endswith("_meta"))
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs an sm_100 GPU (runs through the CUDA library)")
 

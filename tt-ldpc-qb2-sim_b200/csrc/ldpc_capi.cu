@@ -232,6 +232,11 @@ extern "C" int ldpc_kernel_kind(const ldpc_handle* h) {
 
 extern "C" int64_t ldpc_launch_count(const ldpc_handle* h) { return h ? h->launches : -1; }
 
+extern "C" int64_t ldpc_launch_param_bytes(const ldpc_handle* h) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    return h->kind == LDPC_KERNEL_QC ? (int64_t)sizeof(QcParams) : (int64_t)sizeof(GenParams);
+}
+
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int R, int F) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");

@@ -1,0 +1,21 @@
+// Kernel variants for Z = 128, D = 18: AR4JA rate 4/5, K = 4096 (N = 5632, 1536 checks).
+// FP32 message storage is not built for D = 18: 156 fp32 messages per thread do not fit the
+// register file next to the working set (16-bit storage packs them into 78 registers).
+#include "ldpc_qc.cuh"
+#include "ldpc_registry.h"
+
+using namespace ldpcb200;
+
+static const QcEntry qc_r45k4[] = {
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, true, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_NMS, false, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_NMS, true, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, true),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, true),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, true, true),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_NMS, false, true),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_NMS, true, true),
+};
+LDPC_QC_REGISTER(qc_r45k4)

@@ -23,7 +23,7 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
            "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_launch_count",
-           "ldpc_last_error", "ldpc_abi_version")
+           "ldpc_launch_param_bytes", "ldpc_last_error", "ldpc_abi_version")
 
 
 class LdpcError(RuntimeError):
@@ -82,6 +82,8 @@ def load(path: str = LIB_PATH):
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.ldpc_launch_count.argtypes = [C.c_void_p]
     L.ldpc_launch_count.restype = C.c_int64
+    L.ldpc_launch_param_bytes.argtypes = [C.c_void_p]
+    L.ldpc_launch_param_bytes.restype = C.c_int64
     L.ldpc_last_error.argtypes = [C.c_char_p, C.c_size_t]
     L.ldpc_abi_version.argtypes = []
     _lib = L
@@ -171,6 +173,10 @@ class Decoder:
     @property
     def launches(self) -> int:
         return int(self._lib.ldpc_launch_count(self._h))
+
+    @property
+    def launch_param_bytes(self) -> int:
+        return _check(int(self._lib.ldpc_launch_param_bytes(self._h)))
 
     def set_launch_shape(self, rows_per_thread: int = 0, frames_per_cta: int = 0):
         _check(self._lib.ldpc_set_launch_shape(self._h, rows_per_thread, frames_per_cta))

@@ -1,0 +1,289 @@
+"""``ldpc_sim``: the drop-in engine binary behind the reference's ``run_simulation.py``.
+
+Mirrors ``engines/scalar_5w/ldpc_sim_scalar.cpp`` (lines 271-644):
+
+* getopt letters ``c:e:p:t:m:b:k:i:svnL:R:G:V:`` with the same meanings and defaults (``:275-309``):
+  matrix, Eb/N0, punctured count, target frame errors (50), max blocks (0 = k x cores), batch per
+  core (1000), blocks per core (100000), max iterations (16), single core, lockstep verify, NMS, and
+  the L/R/V clips with the proportional G clip (``:357-364``);
+* block accounting over 440 "cores" (1 with ``-s``), so ``run_simulation.py``'s
+  ``max_blocks // 440`` conversion (``run_simulation.py:88-90``) keeps its meaning;
+* the stop rule: whole batches of ``batch x cores`` frames while frame errors < target and
+  blocks < max (``:421-427``);
+* stdout: ``[CONFIG]`` lines, one progress JSON line per batch and the final JSON line with the same
+  keys in the same order (``:618-641``); extra keys are appended after them (the driver ignores
+  them).  Exit status 0; a matrix error prints the message and exits non-zero (the reference throws).
+
+Long options add what the GPU engine offers: ``--storage bf16|fp32|fp16`` (default bf16, the
+reference numerics), ``--seed`` (Philox key, default 133742 like the reference's root seed,
+``:403-407``), ``--device``, ``--out CSV`` (the circulant engine's per-chunk CSV,
+``engines/circulant_dma_4cw/ldpc_sim_circulant_dma.cpp:282-406``) and ``--resume STATE.json``
+(continue a point from its saved frame index and tallies).
+
+Frame f of an Eb/N0 point is decoded from Philox counter (seed, f): every batch takes the next
+``batch x cores`` frame indices, so a run is reproducible and resumable by its frame index.
+"""
+from __future__ import annotations
+
+import getopt
+import json
+import os
+import sys
+import time
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from . import chinn
+
+MESH_CORES = 440  # the reference's 2x2 Blackhole mesh (ldpc_sim_scalar.cpp:318-333)
+DEFAULT_SEED = 133742
+
+
+def _g(x: float) -> str:
+    """A double as C++ iostream prints it by default (6 significant digits, %g)."""
+    s = f"{x:.6g}"
+    if s in ("inf", "-inf", "nan"):
+        return "0"
+    return s
+
+
+def resolve_filepath(name: str) -> str:
+    """ldpc_sim_scalar.cpp:24-30."""
+    for cand in (name, os.path.join("engines", "scalar_5w", name), os.path.join("..", "..", name),
+                 os.path.join("..", name)):
+        if os.path.exists(cand):
+            return cand
+    return name
+
+
+@dataclass
+class Options:
+    matrix: str = ""
+    ebn0: float = 2.0
+    punctured: int = 0
+    target_fe: int = 50
+    blocks_per_core: int = 100000
+    max_blocks: int = 0
+    batch_per_core: int = 1000
+    max_iter: int = 16
+    single_core: bool = False
+    lockstep: bool = False
+    nms: bool = False
+    l_max: float = 0.0
+    r_max: float = 0.0
+    l_post_max: float = 0.0
+    gamma: float = 0.0
+    storage: str = "bf16"
+    seed: int = DEFAULT_SEED
+    device: int = 0
+    out_csv: str = ""
+    resume: str = ""
+    extra: dict = field(default_factory=dict)
+
+
+def parse_args(argv: List[str]) -> Options:
+    o = Options()
+    opts, _ = getopt.gnu_getopt(argv, "c:e:p:t:m:b:k:i:svnL:R:G:V:",
+                                ["storage=", "seed=", "device=", "out=", "resume="])
+    for k, v in opts:
+        if k == "-c": o.matrix = v
+        elif k == "-e": o.ebn0 = float(v)
+        elif k == "-p": o.punctured = int(v)
+        elif k == "-t": o.target_fe = int(v)
+        elif k == "-m": o.max_blocks = int(v)
+        elif k == "-b": o.batch_per_core = int(v)
+        elif k == "-k": o.blocks_per_core = int(v)
+        elif k == "-i": o.max_iter = int(v)
+        elif k == "-s": o.single_core = True
+        elif k == "-v": o.lockstep = True
+        elif k == "-n": o.nms = True
+        elif k == "-L": o.l_max = float(v)
+        elif k == "-R": o.r_max = float(v)
+        elif k == "-V": o.l_post_max = float(v)
+        elif k == "-G": o.gamma = float(v)
+        elif k == "--storage":
+            if v not in ("bf16", "fp32", "fp16"):
+                raise getopt.GetoptError(f"--storage must be bf16, fp32 or fp16, not {v}")
+            o.storage = v
+        elif k == "--seed": o.seed = int(v, 0)
+        elif k == "--device": o.device = int(v)
+        elif k == "--out": o.out_csv = v
+        elif k == "--resume": o.resume = v
+    return o
+
+
+@dataclass
+class Batch:
+    frames: int
+    bit_errors: int
+    frame_errors: int
+    iter_sum: int
+    kernel_ms: float = 0.0
+
+
+class GpuEngine:
+    """The CUDA engine: a ``capi.Decoder`` plus the run parameters of one Eb/N0 point."""
+
+    def __init__(self, mat: chinn.Matrix, punctured: int, device: int):
+        from . import capi
+        self.capi = capi
+        self.dec = capi.Decoder(mat.row_matrix(), mat.N, punctured, device)
+
+    def describe(self) -> str:
+        return "layered QC kernel" if self.dec.kind == self.capi.KERNEL_QC else "general file-order kernel"
+
+    def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
+        p = self.dec.params(mu=mu, sigma=sigma, seed=o.seed, first_frame=first, n_frames=n,
+                            max_iter=o.max_iter, storage=o.storage,
+                            algo=self.capi.ALGO_NMS if o.nms else self.capi.ALGO_AMIN,
+                            l_max=l_max, r_max=o.r_max, l_post_max=o.l_post_max)
+        r = self.dec.run_chunk(p)
+        return Batch(r.frames, r.bit_errors, r.frame_errors, r.iter_sum, r.kernel_ms)
+
+    def close(self):
+        self.dec.close()
+
+
+def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = None, out=None) -> int:
+    out = out or sys.stdout
+    argv = sys.argv[1:] if argv is None else argv
+
+    def say(s: str):
+        out.write(s + "\n")
+        out.flush()
+
+    try:
+        o = parse_args(argv)
+    except (getopt.GetoptError, ValueError) as e:
+        print(f"ldpc_sim: {e}", file=sys.stderr)
+        return 2
+    try:
+        path = resolve_filepath(o.matrix)
+        mat = chinn.parse_chinn(path)
+    except (chinn.MatrixError, OSError, ValueError) as e:
+        print(f"terminate called after throwing an instance of 'std::runtime_error'\n  what():  {e}",
+              file=sys.stderr)
+        return 1
+    say(f"[CONFIG] Matrix loaded: {path} (N={mat.N}, M={mat.M}, max_check_deg={mat.max_check_deg}, "
+        f"max_var_deg={mat.max_var_deg})")
+    if not 0 <= o.punctured < mat.N:
+        print(f"ldpc_sim: punctured count {o.punctured} outside [0, N)", file=sys.stderr)
+        return 1
+    try:
+        engine = (engine_factory or GpuEngine)(mat, o.punctured, o.device)
+    except Exception as e:  # no GPU, library missing, unsupported matrix: fail loudly
+        print(f"ldpc_sim: cannot start the GPU engine: {e}", file=sys.stderr)
+        return 1
+    cores = 1 if o.single_core else MESH_CORES
+    say(f"[CONFIG] Running in {'SINGLE-CORE' if o.single_core else 'MULTI-CORE'} accounting "
+        f"({cores} cores) on one GPU with the {engine.describe()}")
+    max_blocks = o.max_blocks
+    if max_blocks == 0 and o.blocks_per_core > 0:
+        max_blocks = o.blocks_per_core * cores
+    batch = o.batch_per_core
+    if o.blocks_per_core > 0 and batch > o.blocks_per_core:
+        batch = o.blocks_per_core
+    say(f"[CONFIG] Stopping criteria: min {o.target_fe} block errors OR max {o.blocks_per_core} blocks/core "
+        f"(Batch size/core: {batch}, max mesh blocks: {max_blocks}, max iters: {o.max_iter})")
+    say("[CONFIG] Decoder algorithm: " + ("Normalized Min-Sum (alpha=0.75)" if o.nms else
+                                           "Approximate-Min* (Christopher Jones MILCOM 2003)")
+        + f", message storage {o.storage}")
+    rate = (mat.N - mat.M) / (mat.N - o.punctured)
+    snr = 10.0 ** (o.ebn0 / 10.0)
+    mu = float(np.float32(4.0 * rate * snr))
+    sigma = float(np.float32(np.sqrt(8.0 * rate * snr)))
+    l_max = o.l_max
+    if o.gamma > 0.0:
+        l_max = float(np.float32(np.float32(o.gamma) * np.float32(mu)))
+        say(f"[CONFIG] LLR Clipping (Proportional): gamma={_g(o.gamma)} (mu_llr={_g(mu)}) -> "
+            f"L_ch_max={_g(l_max)}, R_max={_g(o.r_max)}, L_post_max={_g(o.l_post_max)}")
+    elif l_max > 0 or o.r_max > 0 or o.l_post_max > 0:
+        say(f"[CONFIG] LLR Clipping (Fixed): L_ch_max={_g(l_max)}, R_max={_g(o.r_max)}, "
+            f"L_post_max={_g(o.l_post_max)}")
+
+    blocks = be = fe = iters = 0
+    kernel_ms = 0.0
+    if o.resume and os.path.exists(o.resume):
+        with open(o.resume) as f:
+            st = json.load(f)
+        if st.get("ebn0") == o.ebn0 and st.get("seed") == o.seed and st.get("matrix") == path:
+            blocks, be, fe, iters = st["blocks"], st["bit_errors"], st["frame_errors"], st.get("iter_sum", 0)
+            say(f"[CONFIG] Resuming at frame {blocks} from {o.resume}")
+
+    csv = None
+    if o.out_csv:
+        exists = os.path.exists(o.out_csv)
+        csv = open(o.out_csv, "a")
+        if not exists:
+            csv.write("EbN0_dB,Total_Blocks,Total_Bit_Errors,Total_Block_Errors,BER,FER,Mean_Iterations,"
+                      "Throughput_Msps,Host_Wall_s\n")
+            csv.flush()
+        say(f" [CSV] Logging to: {o.out_csv}")
+
+    ntx = mat.N - o.punctured
+    t0 = time.perf_counter()
+    try:
+        while fe < o.target_fe and blocks < max_blocks:
+            remaining = max_blocks - blocks
+            cur = batch
+            if remaining < batch * cores:
+                cur = max(1, remaining // cores)
+            total = cur * cores
+            if o.lockstep:
+                # Every core of the reference gets the same generator state (ldpc_sim_scalar.cpp:410-411)
+                # and the host asserts identical stats.  Here the batch's frames are decoded twice by
+                # independent launches and compared; the tallies count all cores' identical copies.
+                # The reference does not advance the generators in this mode: every batch repeats
+                # the same frames (:609-616), so every batch starts at frame 0 here too.
+                a = engine.run(o, mu, sigma, l_max, 0, cur)
+                b2 = engine.run(o, mu, sigma, l_max, 0, cur)
+                same = (a.bit_errors, a.frame_errors, a.iter_sum) == (b2.bit_errors, b2.frame_errors, b2.iter_sum)
+                if same:
+                    say(f"[VERIFICATION PASS] All {cores} cores produced IDENTICAL output: bit_err={a.bit_errors}, "
+                        f"frame_err={a.frame_errors}, iters={a.iter_sum}")
+                else:
+                    print(f"[VERIFICATION FAIL] repeated launches differ: {a} vs {b2}", file=sys.stderr)
+                r = Batch(a.frames * cores, a.bit_errors * cores, a.frame_errors * cores, a.iter_sum * cores,
+                          a.kernel_ms + b2.kernel_ms)
+            else:
+                r = engine.run(o, mu, sigma, l_max, blocks, total)
+            blocks += total
+            be += r.bit_errors
+            fe += r.frame_errors
+            iters += r.iter_sum
+            kernel_ms += r.kernel_ms
+            el = time.perf_counter() - t0
+            ber = be / (blocks * ntx) if blocks else 0.0
+            fer = fe / blocks if blocks else 0.0
+            msps = (blocks * ntx / el) / 1e6 if el > 0 else 0.0
+            say("{" + f"\"progress\": true, \"ebn0\": {_g(o.ebn0)}, \"blocks\": {blocks}, "
+                f"\"max_blocks\": {max_blocks}, \"bit_errors\": {be}, \"frame_errors\": {fe}, "
+                f"\"target_errors\": {o.target_fe}, \"ber\": {_g(ber)}, \"fer\": {_g(fer)}, "
+                f"\"throughput_msps\": {_g(msps)}, \"elapsed_sec\": {_g(el)}, "
+                f"\"mean_iters\": {_g(iters / blocks if blocks else 0.0)}, \"kernel_ms\": {_g(kernel_ms)}" + "}")
+            if csv:
+                csv.write(f"{o.ebn0:.2f},{blocks},{be},{fe},{ber:.6e},{fer:.6e},"
+                          f"{(iters / blocks if blocks else 0.0):.3f},{msps:.2f},{el:.2f}\n")
+                csv.flush()
+            if o.resume:
+                tmp = o.resume + ".tmp"
+                with open(tmp, "w") as f:
+                    json.dump({"matrix": path, "ebn0": o.ebn0, "seed": o.seed, "blocks": blocks,
+                               "bit_errors": be, "frame_errors": fe, "iter_sum": iters}, f)
+                os.replace(tmp, o.resume)
+    finally:
+        if csv:
+            csv.close()
+        close = getattr(engine, "close", None)
+        if close:
+            close()
+    el = time.perf_counter() - t0
+    say("{" + f"\"ebn0\": {_g(o.ebn0)}, \"blocks\": {blocks}, \"bit_errors\": {be}, "
+        f"\"frame_errors\": {fe}, \"elapsed_sec\": {_g(el)}" + "}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
