@@ -136,6 +136,29 @@ int64_t ldpc_launch_count(const ldpc_handle* h);
  * device traffic of ldpc_run_chunk besides the launch itself). */
 int64_t ldpc_launch_param_bytes(const ldpc_handle* h);
 
+/* Size of the device scratch ldpc_decode_llr_static works in (16 MiB per GPU). */
+#define LDPC_STATIC_SCRATCH_BYTES (16u << 20)
+
+/* Decoding without any allocation.  No counterpart in the reference (its workers decode in buffers
+ * the host set up once).  For callers that must not let a library allocate device memory: an
+ * application that reserves all of a GPU's memory up front for its own pool, or one whose device
+ * footprint has to be fixed and known before it runs.  Decodes n_frames frames of the matrix h from
+ * d_llr [n_frames][N-P] fp32 (device memory) into device buffers d_post [n_frames][N], d_iters,
+ * d_synd_fail, d_bit_errors (each may be NULL), on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream), and returns the tallies in *out.  Same decoder and results as ldpc_decode_llr
+ * (the general file-order kernel); no cudaMalloc, cudaFree or host allocation.
+ *
+ * Its scratch (code tables, check messages, claim counter, tallies) is one static device array of
+ * LDPC_STATIC_SCRATCH_BYTES that every GPU loading the library holds until exit.  A matrix needing
+ * more than that for one CTA of 4 frame slots is rejected with LDPC_ENOMEM; larger ones run with as
+ * many frame slots as fit.  The first call on a device looks the array up on that device (make that
+ * first call before any stream capture).  Every call reuses the same array: calls whose work can
+ * overlap on the GPU race and must be serialised by the caller.  The call returns when the work is
+ * done. */
+int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr,
+                           int64_t n_frames, float* d_post, int32_t* d_iters, int32_t* d_synd_fail,
+                           int32_t* d_bit_errors, ldpc_tally* out, void* stream);
+
 /* Copies the last error message of the calling thread into buf (NUL-terminated); returns its
  * length. */
 int ldpc_last_error(char* buf, size_t len);

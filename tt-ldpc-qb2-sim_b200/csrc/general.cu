@@ -1,6 +1,8 @@
 // General-matrix kernel (any parity-check matrix, the reference's file row order) and its host side.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <unordered_set>
 #include <vector>
 
@@ -358,6 +360,218 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
     void* args[] = {&gp};
     cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * GEN_WARPS), args, smem, stream);
     if (e != cudaSuccess) return gfail(err, LDPC_EIO, std::string("general kernel launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+}  // namespace ldpcb200
+
+// ----------------------------------------------------------------------------- no-allocation decode
+//
+// ldpc_decode_llr_static: the general kernel with every byte of its scratch in one file-scope
+// device array, for callers that must not have a library allocate device memory on their GPU (a host
+// application that reserves the whole GPU up front through its own pool, or one that must keep its
+// device footprint fixed and known before it starts).  The caller passes device pointers for the
+// channel LLRs and the outputs; this code calls no cudaMalloc/cudaFree and allocates no host memory.
+//
+// Scratch layout (LDPC_STATIC_SCRATCH_BYTES, 256-byte aligned regions):
+//   [0, 256)           frame-claim counter (u32) and tallies (TALLY_WORDS x u64)
+//   rows               the caller's [M][dmax] row table, copied in
+//   cols               the same table transposed to [dmax][M] (the general kernel's layout)
+//   runs               conflict-free run starts (M + 1 entries) and their count
+//   bitmap             N bits, used while the runs are computed
+//   messages           [slots][dmax][M] check messages, one region per frame slot
+// Every call rewrites the tables and zeroes the counter and tallies; the messages are zeroed by the
+// kernel when it starts a frame.  All calls share the one array, so calls whose work overlaps on the
+// GPU (different streams, or different host threads) race on it: serialise them.
+
+static __device__ __align__(256) unsigned char g_static_scratch[LDPC_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char* g_static_addr[kMaxDevices] = {};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Transposes the row table and splits the file row order into conflict-free runs (the same greedy
+// rule as build_general), one warp, no waits on other threads.
+__global__ void static_setup_kernel(const int32_t* rows, int M, int dmax, int N, int32_t* cols,
+                                    int32_t* runs, int32_t* n_runs, uint32_t* bitmap) {
+    const int lane = threadIdx.x;
+    for (int i = lane; i < M * dmax; i += 32) cols[(i % dmax) * M + i / dmax] = rows[i];
+    for (int w = lane; w < (N + 31) / 32; w += 32) bitmap[w] = 0u;
+    __syncwarp();
+    int nr = 0, start = 0;
+    if (lane == 0) runs[0] = 0;
+    for (int m = 0; m < M; ++m) {
+        const int c = lane < dmax ? rows[(size_t)m * dmax + lane] : -1;
+        const bool clash = c >= 0 && ((bitmap[c >> 5] >> (c & 31)) & 1u);
+        if (__any_sync(0xFFFFFFFFu, clash)) {
+            ++nr;
+            if (lane == 0) runs[nr] = m;
+            for (int r = start; r < m; ++r) {
+                const int c2 = lane < dmax ? rows[(size_t)r * dmax + lane] : -1;
+                if (c2 >= 0) atomicAnd(&bitmap[c2 >> 5], ~(1u << (c2 & 31)));
+            }
+            start = m;
+            __syncwarp();
+        }
+        if (c >= 0) atomicOr(&bitmap[c >> 5], 1u << (c & 31));
+        __syncwarp();
+    }
+    ++nr;
+    if (lane == 0) {
+        runs[nr] = M;
+        *n_runs = nr;
+    }
+}
+
+int sfail(int code, std::string& err, const char* msg) {
+    err = msg;
+    return code;
+}
+
+}  // namespace
+
+namespace ldpcb200 {
+
+int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr, int64_t n,
+                      float* d_post, int32_t* d_iters, int32_t* d_synd, int32_t* d_be, ldpc_tally* out,
+                      cudaStream_t stream, std::string& err) {
+    char msg[256];
+    if (!h || !h->rows || !p) return sfail(LDPC_EINVAL, err, "matrix or params are NULL");
+    if (n < 0 || n > (int64_t)UINT32_MAX) return sfail(LDPC_EINVAL, err, "n_frames out of range");
+    if (n > 0 && !d_llr) return sfail(LDPC_EINVAL, err, "d_llr is NULL");
+    const int N = h->n_vars, M = h->n_checks, P = h->n_punct, dmax = h->max_check_deg;
+    if (N <= 0 || M <= 0 || dmax <= 0 || dmax > 32 || P < 0 || P >= N)
+        return sfail(LDPC_EINVAL, err, "bad matrix dimensions (need N > P >= 0, M > 0, 1 <= max_check_deg <= 32)");
+    if (p->max_iter < 0 || p->storage < 0 || p->storage > 2 || p->algo < 0 || p->algo > 1)
+        return sfail(LDPC_EINVAL, err, "bad run parameters");
+    int maxdeg = 0;
+    for (int64_t i = 0; i < (int64_t)M * dmax; ++i) {
+        const int32_t c = h->rows[i];
+        if (c < -1 || c >= N) return sfail(LDPC_EINVAL, err, "edge index out of bounds");
+        if (c >= 0) maxdeg = std::max(maxdeg, (int)(i % dmax) + 1);
+    }
+    const int dt = maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : 32;
+    const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
+    const size_t rsz = p->storage == STORE_FP32 ? 4 : 2;
+    const size_t off_rows = 256;
+    const size_t off_cols = off_rows + align256((size_t)M * dmax * 4);
+    const size_t off_runs = off_cols + align256((size_t)M * dmax * 4);
+    const size_t off_bits = off_runs + align256((size_t)(M + 2) * 4);
+    const size_t off_msgs = off_bits + align256((size_t)(N + 31) / 32 * 4);
+    const size_t per_slot = (size_t)dmax * M * rsz;
+    if (off_msgs + GEN_WARPS * per_slot > LDPC_STATIC_SCRATCH_BYTES) {
+        snprintf(msg, sizeof msg,
+                 "matrix needs %zu bytes of static scratch for one CTA of %d frame slots; the maximum is %zu",
+                 off_msgs + GEN_WARPS * per_slot, GEN_WARPS, (size_t)LDPC_STATIC_SCRATCH_BYTES);
+        return sfail(LDPC_ENOMEM, err, msg);
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return sfail(LDPC_ENODEV, err, "no current CUDA device");
+    }
+    unsigned char* base;
+    {
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_addr[dev]) {  // once per device, with that device current
+            void* a = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&a, g_static_scratch);
+            if (e != cudaSuccess || !a) {
+                snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+                cudaGetLastError();
+                return sfail(LDPC_EIO, err, msg);
+            }
+            g_static_addr[dev] = static_cast<unsigned char*>(a);
+        }
+        base = g_static_addr[dev];
+    }
+    const void* fn = dt == 8 ? pick_mode<8>(p->storage, p->algo, true)
+                   : dt == 20 ? pick_mode<20>(p->storage, p->algo, true)
+                              : pick_mode<32>(p->storage, p->algo, true);
+    const size_t smem = (size_t)GEN_WARPS * ((N + 7) & ~7) * esz;
+    if (smem > 48 * 1024 && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return sfail(LDPC_ENOTSUP, err, "frame too large for shared memory");
+    }
+    int per_sm = 0, n_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * GEN_WARPS, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0) {
+        cudaGetLastError();
+        return sfail(LDPC_ENOTSUP, err, "general kernel does not fit on an SM");
+    }
+    const uint64_t fit = (LDPC_STATIC_SCRATCH_BYTES - off_msgs) / (GEN_WARPS * per_slot);
+    const uint64_t grid = std::min<uint64_t>({((uint64_t)n + GEN_WARPS - 1) / GEN_WARPS,
+                                              (uint64_t)per_sm * n_sm, fit});
+    unsigned int* d_work = reinterpret_cast<unsigned int*>(base);
+    unsigned long long* d_tally = reinterpret_cast<unsigned long long*>(base + 64);
+    int32_t* d_rows = reinterpret_cast<int32_t*>(base + off_rows);
+    int32_t* d_cols = reinterpret_cast<int32_t*>(base + off_cols);
+    int32_t* d_runs = reinterpret_cast<int32_t*>(base + off_runs);
+    int32_t* d_nruns = d_runs + (M + 1);
+    uint32_t* d_bits = reinterpret_cast<uint32_t*>(base + off_bits);
+    cudaError_t e = cudaMemsetAsync(base, 0, 256, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_rows, h->rows, (size_t)M * dmax * 4, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+        static_setup_kernel<<<1, 32, 0, stream>>>(d_rows, M, dmax, N, d_cols, d_runs, d_nruns, d_bits);
+        e = cudaGetLastError();
+    }
+    int32_t n_runs = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&n_runs, d_nruns, 4, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        snprintf(msg, sizeof msg, "static decode setup: %s", cudaGetErrorString(e));
+        return sfail(LDPC_EIO, err, msg);
+    }
+    if (grid > 0) {
+        GenParams gp;
+        memset(&gp, 0, sizeof gp);
+        gp.cols = d_cols;
+        gp.runs = d_runs;
+        gp.n_runs = n_runs;
+        gp.N = N;
+        gp.M = M;
+        gp.n_tx = N - P;
+        gp.dmax = dmax;
+        gp.max_iter = p->max_iter;
+        gp.l_max = p->l_max;
+        gp.r_max = p->r_max;
+        gp.l_post_max = p->l_post_max;
+        gp.n_frames = (uint32_t)n;
+        gp.r_base = base + off_msgs;
+        gp.llr_in = d_llr;
+        gp.post_out = d_post;
+        gp.iters_out = d_iters;
+        gp.synd_out = d_synd;
+        gp.be_out = d_be;
+        gp.tally = d_tally;
+        gp.hist = nullptr;
+        gp.hist_bins = 1;
+        gp.work = d_work;
+        void* args[] = {&gp};
+        e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * GEN_WARPS), args, smem, stream);
+    }
+    unsigned long long t[TALLY_WORDS] = {};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t, d_tally, sizeof t, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        snprintf(msg, sizeof msg, "static decode: %s", cudaGetErrorString(e));
+        return sfail(LDPC_EIO, err, msg);
+    }
+    if (out) {
+        out->frames = t[T_FRAMES];
+        out->bit_errors = t[T_BIT_ERR];
+        out->frame_errors = t[T_FRAME_ERR];
+        out->iter_sum = t[T_ITER_SUM];
+        out->unconverged = t[T_UNCONVERGED];
+        out->max_iters = t[T_MAX_ITER];
+        out->kernel_ms = 0.0f;
+        out->reserved1 = 0.0f;
+    }
     return 0;
 }
 

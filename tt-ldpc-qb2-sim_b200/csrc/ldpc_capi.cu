@@ -468,6 +468,13 @@ extern "C" int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float*
     return 0;
 }
 
+extern "C" int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr,
+                                      int64_t n, float* d_post, int32_t* d_iters, int32_t* d_synd_fail,
+                                      int32_t* d_bit_errors, ldpc_tally* out, void* stream) {
+    return decode_llr_static(h, p, d_llr, n, d_post, d_iters, d_synd_fail, d_bit_errors, out,
+                             static_cast<cudaStream_t>(stream), g_err);
+}
+
 extern "C" int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins) {
     if (!h || !hist || n_bins <= 0) return fail(LDPC_EINVAL, "bad arguments");
     CU(cudaSetDevice(h->device));

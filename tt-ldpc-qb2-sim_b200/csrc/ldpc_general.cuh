@@ -50,6 +50,10 @@ struct GenParams {
 
 int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCode* g, std::string& err);
 void free_general(GeneralCode* g);
+// No-allocation variant of ldpc_decode_llr (device buffers, static scratch); see general.cu.
+int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr, int64_t n,
+                      float* d_post, int32_t* d_iters, int32_t* d_synd, int32_t* d_be, ldpc_tally* out,
+                      cudaStream_t stream, std::string& err);
 int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                    const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                    unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,

@@ -23,7 +23,7 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
            "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_launch_count",
-           "ldpc_launch_param_bytes", "ldpc_last_error", "ldpc_abi_version")
+           "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
 
 
 class LdpcError(RuntimeError):
@@ -84,6 +84,8 @@ def load(path: str = LIB_PATH):
     L.ldpc_launch_count.restype = C.c_int64
     L.ldpc_launch_param_bytes.argtypes = [C.c_void_p]
     L.ldpc_launch_param_bytes.restype = C.c_int64
+    L.ldpc_decode_llr_static.argtypes = [P(Matrix), P(RunParams), C.c_void_p, C.c_int64, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, P(Tally), C.c_void_p]
     L.ldpc_last_error.argtypes = [C.c_char_p, C.c_size_t]
     L.ldpc_abi_version.argtypes = []
     _lib = L
@@ -116,6 +118,26 @@ def _fp(a):
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32)) if a is not None else None
+
+
+STATIC_SCRATCH_BYTES = 16 << 20
+
+
+def decode_llr_static(rows: np.ndarray, n_vars: int, n_punct: int, p: RunParams, d_llr: int, n_frames: int,
+                      d_post: int = 0, d_iters: int = 0, d_synd_fail: int = 0, d_bit_errors: int = 0,
+                      stream: int = 0) -> "ChunkResult":
+    """ldpc_decode_llr_static: decode frames whose LLRs are already in device memory into device
+    buffers (addresses as integers), with no allocation by the library.  The caller owns every
+    buffer; the library's scratch is a fixed static device array shared by all calls."""
+    lib = load()
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    m = Matrix(int(n_vars), rows.shape[0], int(n_punct), rows.shape[1], _ip(rows))
+    t = Tally()
+    _check(lib.ldpc_decode_llr_static(C.byref(m), C.byref(p), d_llr or None, int(n_frames), d_post or None,
+                                      d_iters or None, d_synd_fail or None, d_bit_errors or None, C.byref(t),
+                                      stream or None))
+    return ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
+                       t.kernel_ms)
 
 
 @dataclass
