@@ -56,7 +56,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--frames", type=int, default=1 << 22, help="frames per Eb/N0 point per GPU per step")
-    ap.add_argument("--storage", choices=("fp32", "fp16", "bf16"), default="fp32")
+    ap.add_argument("--storage", choices=("auto", "fp32", "fp16", "bf16"), default="auto",
+                    help="message storage; auto = the fastest after autotuning")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other storage modes")
@@ -289,6 +291,23 @@ def run_ours(args):
     assert dec.kind == capi.KERNEL_QC
     F = args.frames
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    tuned = {}
+    storage = args.storage
+    if not args.no_autotune:
+        mu25, sigma25 = mu_sigma(code, POINTS[0])
+        res, best = dec.autotune(mu25, sigma25, frames=1 << 18)
+        tuned = {st: {"shape": list(sh), "mframes_per_s": {",".join(map(str, k)): round(v, 3) for k, v in t.items()}}
+                 for st, (sh, t) in res.items()}
+        if storage == "auto":
+            storage = best
+    if storage == "auto":
+        storage = "fp32"
+    if dist:  # every rank runs rank 0's storage choice
+        names = ("fp32", "fp16", "bf16")
+        t = torch.tensor([names.index(storage)], device="cuda")
+        dist.broadcast(t, 0)
+        storage = names[int(t.item())]
+    args.storage = storage
 
     def step(i, storage, acc=None):
         for pi, eb in enumerate(POINTS):
@@ -392,6 +411,7 @@ def run_ours(args):
                 "gsps": round(acc[eb]["frames"] * code.n_tx / (acc[eb]["kernel_ms"] / 1e3) / 1e9, 3)}
                 for eb, v in per_point_tot.items()},
             "storage_comparison": compare,
+            "autotune": tuned,
             "wall_s": round(wall_max, 3),
         },
         "e2e": {"value": round(e2e, 4), "unit": UNIT,
@@ -403,7 +423,7 @@ def run_ours(args):
             "bound": "issue", "unit": "Tlane-op/s",
             "achieved": round(achieved, 3), "peak": round(peak, 3), "frac": round(achieved / peak, 4),
             "traffic": traffic,
-            "kernel": "qc_decode_kernel<128,6,1,1,%s>" % args.storage,
+            "kernel": "qc_decode_kernel<128,6,%s,%s>" % (",".join(map(str, tuned.get(args.storage, {}).get("shape", [1, 1, 0]))), args.storage),
             "work": f"{LANE_OPS_PER_EDGE} lane-ops x {edges} edges x executed iterations; "
                     f"{n_launch_rank0} launches averaging {1e3 * dev_s / max(n_launch_rank0, 1):.2f} ms",
             "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz "

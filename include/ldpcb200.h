@@ -125,9 +125,16 @@ int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);
  * iterations (the last bin also counts every larger value). */
 int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins);
 
-/* Launch shape override for the QC kernel (autotuning): rows per thread and frames per CTA; 0 =
- * automatic.  Returns LDPC_ENOTSUP if that shape is not built for this code. */
-int ldpc_set_launch_shape(ldpc_handle* h, int rows_per_thread, int frames_per_cta);
+/* Launch shape of the QC kernel's simulation path for one storage mode (-1 = all): rows per thread,
+ * frames per CTA, and the resident CTAs per SM its register allocation must allow (a register cap;
+ * 0 = the compiler's choice).  All zero restores the default.  LDPC_ENOTSUP if the shape is not
+ * built for this code.  Used by the autotuner (ldpcb200.capi.Decoder.autotune). */
+int ldpc_set_launch_shape(ldpc_handle* h, int storage, int rows_per_thread, int frames_per_cta,
+                          int min_ctas_per_sm);
+
+/* The QC shapes built for this code and storage mode: writes up to max_shapes triples
+ * (rows per thread, frames per CTA, min CTAs per SM) and returns how many exist. */
+int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes);
 
 /* Number of kernel launches the handle issued since creation (for launch accounting). */
 int64_t ldpc_launch_count(const ldpc_handle* h);

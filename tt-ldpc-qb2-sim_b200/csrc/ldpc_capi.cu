@@ -69,7 +69,7 @@ struct ldpc_handle {
     int Z = 0, D = 0;
     int32_t blk_off[QC_LAYERS][QC_DMAX] = {};
     int32_t shift[QC_LAYERS][QC_DMAX] = {};
-    int force_R = 0, force_F = 0;
+    int shape[3][3] = {};  // per storage mode: rows per thread, frames per CTA, min CTAs/SM (0 = default)
     // general structure (device)
     GeneralCode gen{};
     // device scratch
@@ -237,20 +237,45 @@ extern "C" int64_t ldpc_launch_param_bytes(const ldpc_handle* h) {
     return h->kind == LDPC_KERNEL_QC ? (int64_t)sizeof(QcParams) : (int64_t)sizeof(GenParams);
 }
 
-extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int R, int F) {
+static bool shape_built(const ldpc_handle* h, int storage, int R, int F, int B) {
+    return find_qc(QcKey{h->Z, h->D, R, F, storage, LDPC_ALGO_AMIN, 0, 0, B}) != nullptr;
+}
+
+extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
-    if (R < 0 || F < 0 || F > QC_MAX_F) return fail(LDPC_EINVAL, "bad shape R=%d F=%d", R, F);
-    if (R || F) {
-        QcKey k{h->Z, h->D, R ? R : 1, F ? F : 1, LDPC_STORE_BF16, LDPC_ALGO_AMIN, 0, 0};
-        if (!find_qc(k)) {
-            k.mode = LDPC_STORE_FP32;
-            if (!find_qc(k)) return fail(LDPC_ENOTSUP, "shape R=%d F=%d not built for Z=%d D=%d", R, F, h->Z, h->D);
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0)
+        return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d", storage, R, F, B);
+    const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
+    const int r = R ? R : 1, f = F ? F : 1;
+    bool any = false;
+    for (int s = lo; s <= hi; ++s) any |= shape_built(h, s, r, f, B);
+    if (!any) return fail(LDPC_ENOTSUP, "shape R=%d F=%d B=%d not built for Z=%d D=%d", r, f, B, h->Z, h->D);
+    for (int s = lo; s <= hi; ++s)
+        if (shape_built(h, s, r, f, B) || (R == 0 && F == 0 && B == 0)) {
+            h->shape[s][0] = R;
+            h->shape[s][1] = F;
+            h->shape[s][2] = B;
         }
-    }
-    h->force_R = R;
-    h->force_F = F;
     return 0;
+}
+
+extern "C" int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes) {
+    if (!h || storage < 0 || storage > 2 || (max_shapes > 0 && !shapes)) return fail(LDPC_EINVAL, "bad arguments");
+    if (h->kind != LDPC_KERNEL_QC) return 0;
+    int n = 0;
+    for (const QcTable* t = qc_tables(); t; t = t->next)
+        for (int i = 0; i < t->count; ++i) {
+            const QcKey& k = t->entries[i].key;
+            if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != LDPC_ALGO_AMIN || k.clip || k.ext) continue;
+            if (n < max_shapes) {
+                shapes[3 * n] = k.R;
+                shapes[3 * n + 1] = k.F;
+                shapes[3 * n + 2] = k.B;
+            }
+            ++n;
+        }
+    return n;
 }
 
 static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
@@ -265,23 +290,17 @@ static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
     return 0;
 }
 
-// Launch shape for the QC kernel: rows per thread R, frames per CTA F.
-static void qc_shape(const ldpc_handle* h, int mode, int* R, int* F) {
-    *R = h->force_R ? h->force_R : 1;
-    *F = h->force_F ? h->force_F : 1;
-    (void)mode;
-}
-
 static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                      const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
     const bool clip = p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f;
-    int R, F;
-    qc_shape(h, p->storage, &R, &F);
-    QcKey key{h->Z, h->D, R, F, p->storage, p->algo, clip ? 1 : 0, ext ? 1 : 0};
+    int R = h->shape[p->storage][0] ? h->shape[p->storage][0] : 1;
+    int F = h->shape[p->storage][1] ? h->shape[p->storage][1] : 1;
+    QcKey key{h->Z, h->D, R, F, p->storage, p->algo, clip ? 1 : 0, ext ? 1 : 0, h->shape[p->storage][2]};
     const void* fn = find_qc(key);
-    if (!fn && (R != 1 || F != 1)) {  // fall back to the default shape of the same numerics
+    if (!fn && (R != 1 || F != 1 || key.B != 0)) {  // fall back to the default shape of the same numerics
         key.R = 1;
         key.F = 1;
+        key.B = 0;
         fn = find_qc(key);
         R = F = 1;
     }

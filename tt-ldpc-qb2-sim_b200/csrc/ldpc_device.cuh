@@ -68,4 +68,24 @@ __device__ __forceinline__ float amin_step(float m, float a) {
     return fmaxf(__fsub_rn(cur, corr), 0.0f);
 }
 
+// The same step with the piecewise correction selected by FMA-pipe arithmetic instead of compares
+// and selects (the ALU pipe runs at half the FMA pipe's rate).  Flags f05 = [diff < 0.5] and
+// f2 = [diff < 2] come from saturated fused multiply-adds: 2^30 (0.5 - diff) is >= 32 for every float
+// diff below 0.5 and <= 0 otherwise, so saturation gives exactly 1 or 0.  Then
+//   t = cur - c1*f05,  u = t - c2*(f2 - f05)
+// subtracts exactly one of c1, c2 or nothing, each with one rounding (a product with a 0/1 flag is
+// exact, and adding a signed zero leaves a value unchanged), so the result equals amin_step bit for
+// bit.  Inputs must be finite (c1 * 0 would be NaN for diff = inf): the QC kernel never feeds inf.
+__device__ __forceinline__ float amin_step_fma(float m, float a) {
+    const float diff = fabsf(__fsub_rn(m, a));
+    const float cur = fminf(m, a);
+    const float c1 = __fsub_rn(0.69315f, __fmul_rn(0.40f, diff));
+    const float c2 = __fsub_rn(0.49315f, __fmul_rn(0.328f, __fsub_rn(diff, 0.5f)));
+    const float f05 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 536870912.0f));
+    const float f2 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 2147483648.0f));
+    const float t = __fmaf_rn(-c1, f05, cur);
+    const float u = __fmaf_rn(-c2, __fsub_rn(f2, f05), t);
+    return fmaxf(u, 0.0f);
+}
+
 }  // namespace ldpcb200

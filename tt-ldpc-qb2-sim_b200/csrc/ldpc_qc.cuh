@@ -139,23 +139,23 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         if (ALGO == ALGO_AMIN) {
             // argmin of |q| with a strict < from 9999 (first minimum wins), then the recursive min*
             // over the other edges in row order and a final step with the minimum
-            // (ldpc_decoder_core.h:414-475, 176-201).
-            float mn = 9999.0f;
+            // (ldpc_decoder_core.h:414-475, 176-201).  The other edges in row order are
+            // o_i = |q_i| for i < argmin and |q_{i+1}| after it, so a row of degree d takes d-1 steps.
+            float a[d];
 #pragma unroll
-            for (int e = 0; e < d; ++e) {
-                const float a = fabsf(q[f][e]);
-                const bool lt = a < mn;
-                mn = lt ? a : mn;
+            for (int e = 0; e < d; ++e) a[e] = fabsf(q[f][e]);
+            float mn = fminf(a[0], 9999.0f);
+#pragma unroll
+            for (int e = 1; e < d; ++e) {
+                const bool lt = a[e] < mn;
+                mn = lt ? a[e] : mn;
                 am = lt ? e : am;
             }
-            float m = __int_as_float(0x7f800000);
+            float m = (0 < am) ? a[0] : a[1];
 #pragma unroll
-            for (int e = 0; e < d; ++e) {
-                const float nm = amin_step(m, fabsf(q[f][e]));
-                m = (e == am) ? m : nm;
-            }
+            for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, (i < am) ? a[i] : a[i + 1]);
             mag_min = m;
-            mag_all = amin_step(m, mn);
+            mag_all = amin_step_fma(m, mn);
         } else {
             // normalised min-sum, alpha = 0.75 (ldpc_decoder_core.h:322-379)
             float m1 = 999.0f, m2 = 999.0f;
@@ -191,8 +191,10 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
     }
 }
 
-template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT>
-__global__ void __launch_bounds__(Z / R) qc_decode_kernel(const __grid_constant__ QcParams p) {
+// B: resident CTAs per SM the register allocation must allow (0 = the compiler's choice); a larger B
+// caps registers per thread at 65536 / (B * Z/R) and trades registers for resident warps.
+template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0>
+__global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
     static_assert(Z % 32 == 0 && Z % R == 0 && T % 32 == 0, "Z must be a multiple of 32 and of 32*R");
@@ -207,7 +209,6 @@ __global__ void __launch_bounds__(Z / R) qc_decode_kernel(const __grid_constant_
     LE* sL = reinterpret_cast<LE*>(smem_raw);
     uint32_t* sHB = reinterpret_cast<uint32_t*>(smem_raw + (size_t)F * lstride * sizeof(LE));  // [F][nblk*W]
     __shared__ uint32_t s_fid[QC_MAX_F];
-    __shared__ uint32_t s_fail;
     __shared__ uint32_t s_sfail[QC_MAX_F];
     __shared__ uint32_t s_be[QC_MAX_F];
 

@@ -7,10 +7,10 @@
 namespace ldpcb200 {
 
 struct QcKey {
-    int Z, D, R, F, mode, algo, clip, ext;
+    int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
     bool operator==(const QcKey& o) const {
         return Z == o.Z && D == o.D && R == o.R && F == o.F && mode == o.mode && algo == o.algo &&
-               clip == o.clip && ext == o.ext;
+               clip == o.clip && ext == o.ext && B == o.B;
     }
 };
 
@@ -31,9 +31,10 @@ const QcTable* qc_tables();
 
 }  // namespace ldpcb200
 
-#define LDPC_QC_ENTRY(Z, D, R, F, MODE, ALGO, CLIP, EXT)                       \
-    {{Z, D, R, F, MODE, ALGO, CLIP, EXT},                                      \
-     reinterpret_cast<const void*>(&::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT>)}
+#define LDPC_QC_ENTRY(Z, D, R, F, MODE, ALGO, CLIP, EXT) LDPC_QC_ENTRY_B(Z, D, R, F, MODE, ALGO, CLIP, EXT, 0)
+#define LDPC_QC_ENTRY_B(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                  \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B},                                   \
+     reinterpret_cast<const void*>(&::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B>)}
 
 #define LDPC_QC_REGISTER(name)                                                           \
     namespace {                                                                          \

@@ -12,6 +12,15 @@ static const QcEntry qc_r12k1[] = {
     LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP32, ALGO_AMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP16, ALGO_AMIN, false, false),
+    // register caps for more resident warps: 5 CTAs/SM (<= 96 registers), 6 (<= 80), 8 (<= 64)
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 5),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 6),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 5),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 6),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 5),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 6),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8),
     // caller-supplied LLRs (parity tests, ldpc_decode_llr)
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, true),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, true),

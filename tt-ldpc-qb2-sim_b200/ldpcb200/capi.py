@@ -22,7 +22,7 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
-           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_launch_count",
+           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_list_shapes", "ldpc_launch_count",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
 
 
@@ -79,7 +79,8 @@ def load(path: str = LIB_PATH):
                                   P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
     L.ldpc_channel_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float)]
     L.ldpc_iter_histogram.argtypes = [C.c_void_p, P(C.c_uint64), C.c_int]
-    L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_launch_count.argtypes = [C.c_void_p]
     L.ldpc_launch_count.restype = C.c_int64
     L.ldpc_launch_param_bytes.argtypes = [C.c_void_p]
@@ -200,8 +201,43 @@ class Decoder:
     def launch_param_bytes(self) -> int:
         return _check(int(self._lib.ldpc_launch_param_bytes(self._h)))
 
-    def set_launch_shape(self, rows_per_thread: int = 0, frames_per_cta: int = 0):
-        _check(self._lib.ldpc_set_launch_shape(self._h, rows_per_thread, frames_per_cta))
+    def set_launch_shape(self, rows_per_thread: int = 0, frames_per_cta: int = 0, min_ctas_per_sm: int = 0,
+                         storage=-1):
+        if isinstance(storage, str):
+            storage = STORAGE_NAMES[storage]
+        _check(self._lib.ldpc_set_launch_shape(self._h, storage, rows_per_thread, frames_per_cta, min_ctas_per_sm))
+
+    def shapes(self, storage) -> list:
+        """Built QC launch shapes (rows per thread, frames per CTA, min CTAs per SM) for a storage mode."""
+        if isinstance(storage, str):
+            storage = STORAGE_NAMES[storage]
+        buf = np.zeros(3 * 64, np.int32)
+        n = _check(self._lib.ldpc_list_shapes(self._h, storage, _ip(buf), 64))
+        return [tuple(int(x) for x in buf[3 * i:3 * i + 3]) for i in range(min(n, 64))]
+
+    def autotune(self, mu: float, sigma: float, storages=("fp32", "fp16", "bf16"), frames: int = 1 << 18,
+                 max_iter: int = 200, seed: int = 0x5EED, repeats: int = 2):
+        """Times every built launch shape of each storage mode on ``frames`` frames of this channel
+        and keeps the fastest per mode.  Returns {storage: (best shape, {shape: Mframes/s})} and the
+        fastest storage overall."""
+        out = {}
+        best_overall = None
+        for st in storages:
+            shapes = self.shapes(st) if self.kind == KERNEL_QC else []
+            timings = {}
+            for sh in shapes:
+                self.set_launch_shape(*sh, storage=st)
+                p = self.params(mu=mu, sigma=sigma, seed=seed, n_frames=frames, max_iter=max_iter, storage=st)
+                self.run_chunk(p)  # warm-up
+                ms = min(self.run_chunk(p).kernel_ms for _ in range(repeats))
+                timings[sh] = frames / (ms * 1e-3) / 1e6
+            if timings:
+                best = max(timings, key=timings.get)
+                self.set_launch_shape(*best, storage=st)
+                out[st] = (best, timings)
+                if best_overall is None or timings[best] > out[best_overall][1][out[best_overall][0]]:
+                    best_overall = st
+        return out, best_overall
 
     @staticmethod
     def params(mu=0.0, sigma=0.0, seed=1, stream=0, first_frame=0, n_frames=0, max_iter=200,
