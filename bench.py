@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--storage", choices=("auto", "fp32", "fp16", "bf16"), default="auto",
                     help="message storage; auto = the fastest after autotuning")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--shape", default="", help="R,F,B launch shape for --storage (implies --no-autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other storage modes")
@@ -293,7 +294,12 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     tuned = {}
     storage = args.storage
-    if not args.no_autotune:
+    if args.shape:
+        if storage == "auto":
+            storage = "fp32"
+        dec.set_launch_shape(*[int(x) for x in args.shape.split(",")], storage=storage)
+        tuned = {storage: {"shape": [int(x) for x in args.shape.split(",")], "mframes_per_s": {}}}
+    elif not args.no_autotune:
         mu25, sigma25 = mu_sigma(code, POINTS[0])
         res, best = dec.autotune(mu25, sigma25, frames=1 << 18)
         tuned = {st: {"shape": list(sh), "mframes_per_s": {",".join(map(str, k)): round(v, 3) for k, v in t.items()}}

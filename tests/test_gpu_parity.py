@@ -124,3 +124,57 @@ def test_chunking_is_deterministic(dec_r12k1):
     assert whole.frames == 2000
     for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged"):
         assert getattr(whole, k) == getattr(a, k) + getattr(b, k)
+
+
+@pytest.mark.parametrize("storage", ["bf16", "fp16"])
+@pytest.mark.parametrize("n", [1, 23])
+def test_paired_kernel_matches_oracle(dec_r12k1, storage, n):
+    """Two interleaved frames per thread with packed f32x2 arithmetic: the same bits as the oracle
+    (and as the one-frame kernel), including a pair left half-empty by an odd frame count."""
+    c = ar4ja.make_code(1024, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.0)
+    rng = np.random.default_rng(7 + n)
+    llr = (mu + sigma * rng.standard_normal((n, c.n_tx))).astype(np.float32)
+    dec_r12k1.set_launch_shape(1, 2, 0, storage=storage)
+    try:
+        post, it, sf, be, tal = dec_r12k1.decode_llr(llr, max_iter=60, storage=storage)
+    finally:
+        dec_r12k1.set_launch_shape(0, 0, 0, storage=storage)
+    mode = {"bf16": O.STORE_BF16, "fp16": O.STORE_FP16}[storage]
+    opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=60)
+    assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
+    assert np.array_equal(_bits(post), _bits(opost))
+
+
+def test_paired_kernel_on_reference_golden(golden, dec_r12k1):
+    """The paired kernel on every fixture case of the reference worker it supports (rate 1/2
+    K=1024 in makeH order, Approximate-Min*, no clips): the reference's bits."""
+    dec_r12k1.set_launch_shape(1, 2, 0, storage="bf16")
+    try:
+        n = 0
+        for case in golden["cases"]:
+            if case["matrix"] != "makeh_r12_k1024" or case["nms"] or case["l_max"] or case["r_max"] \
+                    or case["l_post_max"]:
+                continue
+            frames, want, post, it, sf, be, tal = _run_case(dec_r12k1, case)
+            assert np.array_equal(_bits(post), _bits(want)), case["name"]
+            n += 1
+        assert n >= 10
+    finally:
+        dec_r12k1.set_launch_shape(0, 0, 0, storage="bf16")
+
+
+@pytest.mark.parametrize("storage", ["bf16", "fp16"])
+def test_paired_sim_path_equals_single(dec_r12k1, storage):
+    """Fused simulation path: the paired kernel's tallies equal the one-frame kernel's on the same
+    frames (same channel, same decoder bits)."""
+    mu, sigma = capi.channel_mu_sigma(2560, 1536, 512, 1.5)
+    p = dec_r12k1.params(mu=mu, sigma=sigma, seed=3, first_frame=77, n_frames=5001, max_iter=200, storage=storage)
+    single = dec_r12k1.run_chunk(p)
+    dec_r12k1.set_launch_shape(1, 2, 0, storage=storage)
+    try:
+        paired = dec_r12k1.run_chunk(p)
+    finally:
+        dec_r12k1.set_launch_shape(0, 0, 0, storage=storage)
+    for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters"):
+        assert getattr(single, k) == getattr(paired, k), k

@@ -134,39 +134,47 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
 #pragma unroll
         for (int e = 0; e < d; ++e) par ^= __float_as_uint(q[f][e]);
         par &= 0x80000000u;
-        int am = 0;
+        float a[d];
+#pragma unroll
+        for (int e = 0; e < d; ++e) a[e] = fabsf(q[f][e]);
+        // is_am[e]: edge e is the argmin of |q| with a strict < from the reference's initial values
+        // (9999 for Approximate-Min*, 999 for min-sum), the first minimum winning.
+        bool is_am[d];
         float mag_min, mag_all;
         if (ALGO == ALGO_AMIN) {
-            // argmin of |q| with a strict < from 9999 (first minimum wins), then the recursive min*
-            // over the other edges in row order and a final step with the minimum
-            // (ldpc_decoder_core.h:414-475, 176-201).  The other edges in row order are
-            // o_i = |q_i| for i < argmin and |q_{i+1}| after it, so a row of degree d takes d-1 steps.
-            float a[d];
+            // Prefix minima pm_i = min(9999, |q_0|, .., |q_i|); mn = pm_{d-1}.  The argmin index am is
+            // the first i with |q_i| = mn, so i < am exactly when pm_i > mn: no index is tracked.
+            // The other edges in row order are o_i = |q_i| for i < am and |q_{i+1}| after it, and the
+            // recursive min* (ldpc_decoder_core.h:176-201) over them takes d-2 steps, then one final
+            // step with mn (d-1 steps in all).
+            float pm[d];
+            pm[0] = fminf(a[0], 9999.0f);
 #pragma unroll
-            for (int e = 0; e < d; ++e) a[e] = fabsf(q[f][e]);
-            float mn = fminf(a[0], 9999.0f);
+            for (int e = 1; e < d; ++e) pm[e] = fminf(pm[e - 1], a[e]);
+            const float mn = pm[d - 1];
+            bool lt[d];  // lt[i] = (i < am)
 #pragma unroll
-            for (int e = 1; e < d; ++e) {
-                const bool lt = a[e] < mn;
-                mn = lt ? a[e] : mn;
-                am = lt ? e : am;
-            }
-            float m = (0 < am) ? a[0] : a[1];
+            for (int i = 0; i < d; ++i) lt[i] = (i + 1 < d) ? (pm[i] > mn) : false;
 #pragma unroll
-            for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, (i < am) ? a[i] : a[i + 1]);
+            for (int e = 0; e < d; ++e) is_am[e] = (e == 0 ? true : lt[e - 1]) && !lt[e];
+            float m = lt[0] ? a[0] : a[1];
+#pragma unroll
+            for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, lt[i] ? a[i] : a[i + 1]);
             mag_min = m;
             mag_all = amin_step_fma(m, mn);
         } else {
             // normalised min-sum, alpha = 0.75 (ldpc_decoder_core.h:322-379)
+            int am = 0;
             float m1 = 999.0f, m2 = 999.0f;
 #pragma unroll
             for (int e = 0; e < d; ++e) {
-                const float a = fabsf(q[f][e]);
-                const bool l1 = a < m1, l2 = a < m2;
-                m2 = l1 ? m1 : (l2 ? a : m2);
+                const bool l1 = a[e] < m1, l2 = a[e] < m2;
+                m2 = l1 ? m1 : (l2 ? a[e] : m2);
                 am = l1 ? e : am;
-                m1 = l1 ? a : m1;
+                m1 = l1 ? a[e] : m1;
             }
+#pragma unroll
+            for (int e = 0; e < d; ++e) is_am[e] = (e == am);
             mag_min = __fmul_rn(0.75f, m2);
             mag_all = __fmul_rn(0.75f, m1);
         }
@@ -180,7 +188,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         float rn[d];
 #pragma unroll
         for (int e = 0; e < d; ++e) {
-            const uint32_t sel = (e == am) ? smin : sall;
+            const uint32_t sel = is_am[e] ? smin : sall;
             rn[e] = __uint_as_float(sel ^ (__float_as_uint(q[f][e]) & 0x80000000u));
             float ln = __fadd_rn(q[f][e], rn[e]);
             if (CLIP) ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
@@ -191,14 +199,171 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Paired mode: two frame slots per thread in lockstep, interleaved per variable in shared memory
+// (element i of slot f at index 2i + f), so one address, one shared-memory access and one packed
+// f32x2 instruction (FFMA2/FADD2/FMUL2) serve both frames.  Messages stay in registers, one 32-bit
+// word per edge holding both frames' 16-bit values (bf16 or fp16).  Results equal the unpaired
+// kernel bit for bit: every packed operation rounds each lane exactly like its scalar form.
+
+template <int d, int MODE> struct RowMsgPair {  // w[e]: slot 0 in bits 15:0, slot 1 in bits 31:16
+    uint32_t w[d];
+    __device__ __forceinline__ void zero_slot(int f) {
+#pragma unroll
+        for (int e = 0; e < d; ++e) w[e] &= f ? 0x0000FFFFu : 0xFFFF0000u;
+    }
+    __device__ __forceinline__ float2 get2(int e) const {
+        const uint32_t x = w[e];
+        if (MODE == STORE_BF16) return make_float2(__uint_as_float(x << 16), __uint_as_float(x & 0xFFFF0000u));
+        return __half22float2(*reinterpret_cast<const __half2*>(&x));
+    }
+    __device__ __forceinline__ void set2(int e, float2 v) {
+        uint32_t x;
+        if (MODE == STORE_BF16) {
+            __nv_bfloat162 b = __floats2bfloat162_rn(v.x, v.y);
+            x = *reinterpret_cast<uint32_t*>(&b);
+        } else {  // IEEE fp16 with saturation at +-65504, both lanes in one conversion
+            asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(x) : "f"(v.y), "f"(v.x));
+        }
+        w[e] = x;
+    }
+};
+
+template <int MODE> __device__ __forceinline__ float2 ld_pair(const typename LTraits<MODE>::T* sL, int i) {
+    if constexpr (MODE == STORE_BF16) {
+        const uint32_t x = reinterpret_cast<const uint32_t*>(sL)[i];
+        return make_float2(__uint_as_float(x << 16), __uint_as_float(x & 0xFFFF0000u));
+    } else {
+        return reinterpret_cast<const float2*>(sL)[i];
+    }
+}
+template <int MODE> __device__ __forceinline__ void st_pair(typename LTraits<MODE>::T* sL, int i, float2 v) {
+    if constexpr (MODE == STORE_BF16) {
+        __nv_bfloat162 b = __floats2bfloat162_rn(v.x, v.y);
+        reinterpret_cast<uint32_t*>(sL)[i] = *reinterpret_cast<uint32_t*>(&b);
+    } else {
+        reinterpret_cast<float2*>(sL)[i] = v;
+    }
+}
+
+// amin_step_fma on two independent lanes, its FMA-pipe arithmetic as packed f32x2 operations.
+// m, a >= 0 and finite.  diff = max(m,a) - min(m,a) is |m - a| exactly; c1n = 0.4 diff - 0.69315 and
+// c2n = 0.328 (diff - 0.5) - 0.49315 are the negated corrections (round-to-nearest is symmetric).
+__device__ __forceinline__ float2 amin_step_pair(float2 m, float2 a) {
+    const float2 one = make_float2(1.0f, 1.0f), neg1 = make_float2(-1.0f, -1.0f);
+    const float2 cur = make_float2(fminf(m.x, a.x), fminf(m.y, a.y));
+    const float2 mx = make_float2(fmaxf(m.x, a.x), fmaxf(m.y, a.y));
+    const float2 diff = __ffma2_rn(cur, neg1, mx);
+    const float2 c1n = __ffma2_rn(__fmul2_rn(diff, make_float2(0.40f, 0.40f)), one, make_float2(-0.69315f, -0.69315f));
+    const float2 c2n = __ffma2_rn(__fmul2_rn(__fadd2_rn(diff, make_float2(-0.5f, -0.5f)), make_float2(0.328f, 0.328f)),
+                                  one, make_float2(-0.49315f, -0.49315f));
+    const float2 f05 = make_float2(__saturatef(__fmaf_rn(diff.x, -1073741824.0f, 536870912.0f)),
+                                   __saturatef(__fmaf_rn(diff.y, -1073741824.0f, 536870912.0f)));
+    const float2 f2 = make_float2(__saturatef(__fmaf_rn(diff.x, -1073741824.0f, 2147483648.0f)),
+                                  __saturatef(__fmaf_rn(diff.y, -1073741824.0f, 2147483648.0f)));
+    const float2 g = __ffma2_rn(f05, neg1, f2);
+    const float2 t = __ffma2_rn(c1n, f05, cur);
+    const float2 u = __ffma2_rn(c2n, g, t);
+    return make_float2(fmaxf(u.x, 0.0f), fmaxf(u.y, 0.0f));
+}
+
+// One row of degree d for both slots of a pair (Approximate-Min*, no clips).
+template <int d, int MODE>
+__device__ __forceinline__ void row_update_pair(const int (&idx)[d], typename LTraits<MODE>::T* sL,
+                                                RowMsgPair<d, MODE>& rm) {
+    float2 q[d];
+#pragma unroll
+    for (int e = 0; e < d; ++e) q[e] = __ffma2_rn(rm.get2(e), make_float2(-1.0f, -1.0f), ld_pair<MODE>(sL, idx[e]));
+    uint32_t par0 = 0, par1 = 0;
+#pragma unroll
+    for (int e = 0; e < d; ++e) {
+        par0 ^= __float_as_uint(q[e].x);
+        par1 ^= __float_as_uint(q[e].y);
+    }
+    par0 &= 0x80000000u;
+    par1 &= 0x80000000u;
+    float pm0[d], pm1[d];
+    pm0[0] = fminf(fabsf(q[0].x), 9999.0f);
+    pm1[0] = fminf(fabsf(q[0].y), 9999.0f);
+#pragma unroll
+    for (int e = 1; e < d; ++e) {
+        pm0[e] = fminf(pm0[e - 1], fabsf(q[e].x));
+        pm1[e] = fminf(pm1[e - 1], fabsf(q[e].y));
+    }
+    const float2 mn = make_float2(pm0[d - 1], pm1[d - 1]);
+    bool lt0[d], lt1[d];
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+        lt0[i] = (i + 1 < d) ? (pm0[i] > mn.x) : false;
+        lt1[i] = (i + 1 < d) ? (pm1[i] > mn.y) : false;
+    }
+    float2 m = make_float2(fabsf(lt0[0] ? q[0].x : q[1].x), fabsf(lt1[0] ? q[0].y : q[1].y));
+#pragma unroll
+    for (int i = 1; i + 1 < d; ++i)
+        m = amin_step_pair(m, make_float2(fabsf(lt0[i] ? q[i].x : q[i + 1].x), fabsf(lt1[i] ? q[i].y : q[i + 1].y)));
+    const float2 mall = amin_step_pair(m, mn);
+    const uint32_t smin0 = __float_as_uint(m.x) | par0, sall0 = __float_as_uint(mall.x) | par0;
+    const uint32_t smin1 = __float_as_uint(m.y) | par1, sall1 = __float_as_uint(mall.y) | par1;
+#pragma unroll
+    for (int e = 0; e < d; ++e) {
+        const bool am0 = (e == 0 ? true : lt0[e - 1]) && !lt0[e];
+        const bool am1 = (e == 0 ? true : lt1[e - 1]) && !lt1[e];
+        const float2 rn = make_float2(__uint_as_float((am0 ? smin0 : sall0) ^ (__float_as_uint(q[e].x) & 0x80000000u)),
+                                      __uint_as_float((am1 ? smin1 : sall1) ^ (__float_as_uint(q[e].y) & 0x80000000u)));
+        st_pair<MODE>(sL, idx[e], __fadd2_rn(q[e], rn));
+        rm.set2(e, rn);
+    }
+}
+
+// Element i of frame slot f: slot-major (f * lstride + i) or interleaved in pairs (2i + f).
+template <int MODE, bool PAIR> struct SlotView {
+    typename LTraits<MODE>::T* p;
+    __device__ __forceinline__ SlotView(typename LTraits<MODE>::T* base, int f, int lstride)
+        : p(PAIR ? base + f : base + (size_t)f * lstride) {}
+    __device__ __forceinline__ int at(int i) const { return PAIR ? 2 * i : i; }
+    __device__ __forceinline__ float ld(int i) const { return LTraits<MODE>::ld(p, at(i)); }
+    __device__ __forceinline__ void st(int i, float v) const { LTraits<MODE>::st(p, at(i), v); }
+    __device__ __forceinline__ uint32_t sign(int i) const { return LTraits<MODE>::sign(p, at(i)); }
+};
+
+// Registers holding the messages of one CTA's rows: [layer][row][slot] rows, or one pair per row.
+template <int D, int R, int F, int MODE, bool PAIR> struct MsgRegs {
+    RowMsg<QC_DEG_LOW, MODE> r3[4][R][F];
+    RowMsg<D, MODE> rD[8][R][F];
+    __device__ __forceinline__ void zero_slot(int f) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l)
+#pragma unroll
+            for (int rho = 0; rho < R; ++rho) r3[l][rho][f].zero();
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+#pragma unroll
+            for (int rho = 0; rho < R; ++rho) rD[l][rho][f].zero();
+    }
+};
+template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, true> {
+    RowMsgPair<QC_DEG_LOW, MODE> r3[4];
+    RowMsgPair<D, MODE> rD[8];
+    __device__ __forceinline__ void zero_slot(int f) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) r3[l].zero_slot(f);
+#pragma unroll
+        for (int l = 0; l < 8; ++l) rD[l].zero_slot(f);
+    }
+};
+
 // B: resident CTAs per SM the register allocation must allow (0 = the compiler's choice); a larger B
 // caps registers per thread at 65536 / (B * Z/R) and trades registers for resident warps.
-template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0>
+// PAIR: the paired mode above (F = 2, R = 1, 16-bit storage, Approximate-Min*, no clips).
+template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
     static_assert(Z % 32 == 0 && Z % R == 0 && T % 32 == 0, "Z must be a multiple of 32 and of 32*R");
     static_assert(F >= 1 && F <= QC_MAX_F, "frames per CTA");
+    static_assert(!PAIR || (F == 2 && R == 1 && MODE != STORE_FP32 && ALGO == ALGO_AMIN && !CLIP),
+                  "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
+    using SV = SlotView<MODE, PAIR>;
     using LT = LTraits<MODE>;
     using LE = typename LT::T;
 
@@ -217,8 +382,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
 
-    RowMsg<QC_DEG_LOW, MODE> r3[4][R][F];
-    RowMsg<D, MODE> rD[8][R][F];
+    MsgRegs<D, R, F, MODE, PAIR> msg;
 
     uint32_t act = 0;                // active slots (uniform)
     uint32_t need = (1u << F) - 1u;  // slots waiting for a frame (uniform)
@@ -249,15 +413,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 it[f] = 0;
                 if (fid[f] == 0xFFFFFFFFu) { act &= ~(1u << f); continue; }
                 act |= 1u << f;
-#pragma unroll
-                for (int l = 0; l < 4; ++l)
-#pragma unroll
-                    for (int rho = 0; rho < R; ++rho) r3[l][rho][f].zero();
-#pragma unroll
-                for (int l = 0; l < 8; ++l)
-#pragma unroll
-                    for (int rho = 0; rho < R; ++rho) rD[l][rho][f].zero();
-                LE* L = sL + f * lstride;
+                msg.zero_slot(f);
+                const SV L(sL, f, lstride);
                 const int nq = p.n_tx >> 2;
                 if (EXT) {
                     const float4* src = reinterpret_cast<const float4*>(p.llr_in + (size_t)fid[f] * p.n_tx);
@@ -268,7 +425,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         for (int k = 0; k < 4; ++k) {
                             float x = v[k];
                             if (CLIP && p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
-                            LT::st(L, 4 * qd + k, x);
+                            L.st(4 * qd + k, x);
                         }
                     }
                 } else {
@@ -287,11 +444,11 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         for (int k = 0; k < 4; ++k) {
                             float x = p.sigma > 0.0f ? __fmaf_rn(p.sigma, n[k], p.mu) : p.mu;
                             if (CLIP && p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
-                            LT::st(L, 4 * qd + k, x);
+                            L.st(4 * qd + k, x);
                         }
                     }
                 }
-                for (int i = p.n_tx + tid; i < N; i += T) LT::st(L, i, 0.0f);
+                for (int i = p.n_tx + tid; i < N; i += T) L.st(i, 0.0f);
             }
             need = 0;
             __syncthreads();
@@ -309,12 +466,18 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         int idx[QC_DEG_LOW];
 #pragma unroll
                         for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
-                        row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, r3[l & 3][rho], r_cap, lp_cap);
+                        if constexpr (PAIR)
+                            row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
+                        else
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap);
                     } else {
                         int idx[D];
 #pragma unroll
                         for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
-                        row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rD[(l - 4) & 7][rho], r_cap, lp_cap);
+                        if constexpr (PAIR)
+                            row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
+                        else
+                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap, lp_cap);
                     }
                 }
                 __syncthreads();
@@ -335,10 +498,10 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
 #pragma unroll
         for (int f = 0; f < F; ++f) {
             if (!((eval >> f) & 1u)) continue;
-            const LE* L = sL + f * lstride;
+            const SV L(sL, f, lstride);
             uint32_t* hb = sHB + f * nwords;
             for (int wd = warp; wd < nwords; wd += T / 32) {
-                const uint32_t b = __ballot_sync(0xFFFFFFFFu, LT::sign(L, wd * 32 + lane));
+                const uint32_t b = __ballot_sync(0xFFFFFFFFu, L.sign(wd * 32 + lane));
                 if (lane == 0) hb[wd] = b;
             }
         }
@@ -399,9 +562,9 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 if (p.be_out) p.be_out[fid[f]] = (int32_t)be;
             }
             if (p.post_out) {
-                const LE* L = sL + f * lstride;
+                const SV L(sL, f, lstride);
                 float* dst = p.post_out + (size_t)fid[f] * N;
-                for (int i = tid; i < N; i += T) dst[i] = LT::ld(L, i);
+                for (int i = tid; i < N; i += T) dst[i] = L.ld(i);
             }
         }
         need = done;

@@ -8,6 +8,8 @@ namespace ldpcb200 {
 
 struct QcKey {
     int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
+    // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
+    // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
         return Z == o.Z && D == o.D && R == o.R && F == o.F && mode == o.mode && algo == o.algo &&
                clip == o.clip && ext == o.ext && B == o.B;
@@ -35,6 +37,11 @@ const QcTable* qc_tables();
 #define LDPC_QC_ENTRY_B(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                  \
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B},                                   \
      reinterpret_cast<const void*>(&::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B>)}
+
+#define LDPC_QC_ENTRY_PAIR(Z, D, MODE, EXT, B)                                 \
+    {{Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, 0, EXT, B},                     \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, false, EXT, B, true>)}
 
 #define LDPC_QC_REGISTER(name)                                                           \
     namespace {                                                                          \

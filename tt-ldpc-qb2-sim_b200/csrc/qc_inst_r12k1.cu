@@ -7,11 +7,18 @@ using namespace ldpcb200;
 static const QcEntry qc_r12k1[] = {
     // simulation (Philox channel), Approximate-Min*, no clips: the benchmarked path
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false),
-    LDPC_QC_ENTRY(128, 6, 1, 2, STORE_BF16, ALGO_AMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP32, ALGO_AMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false),
-    LDPC_QC_ENTRY(128, 6, 1, 2, STORE_FP16, ALGO_AMIN, false, false),
+    // paired: two interleaved frames per thread, packed f32x2 arithmetic (16-bit messages)
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_BF16, false, 0),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_BF16, false, 4),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_BF16, false, 5),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_FP16, false, 0),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_FP16, false, 4),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_FP16, false, 5),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_BF16, true, 0),
+    LDPC_QC_ENTRY_PAIR(128, 6, STORE_FP16, true, 0),
     // register caps for more resident warps: 5 CTAs/SM (<= 96 registers), 6 (<= 80), 8 (<= 64)
     LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 5),
     LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 6),
