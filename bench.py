@@ -59,7 +59,7 @@ def parse_args():
     ap.add_argument("--storage", choices=("auto", "fp32", "fp16", "bf16"), default="auto",
                     help="message storage; auto = the fastest after autotuning")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--shape", default="", help="R,F,B launch shape for --storage (implies --no-autotune)")
+    ap.add_argument("--shape", default="", help="R,F,B[,G] launch shape for --storage (implies --no-autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other storage modes")
@@ -429,7 +429,7 @@ def run_ours(args):
             "bound": "issue", "unit": "Tlane-op/s",
             "achieved": round(achieved, 3), "peak": round(peak, 3), "frac": round(achieved / peak, 4),
             "traffic": traffic,
-            "kernel": "qc_decode_kernel<128,6,%s,%s>" % (",".join(map(str, tuned.get(args.storage, {}).get("shape", [1, 1, 0]))), args.storage),
+            "kernel": "qc_decode_kernel<128,6,%s,%s>" % (",".join(map(str, tuned.get(args.storage, {}).get("shape", [1, 1, 0, 0]))), args.storage),
             "work": f"{LANE_OPS_PER_EDGE} lane-ops x {edges} edges x executed iterations; "
                     f"{n_launch_rank0} launches averaging {1e3 * dev_s / max(n_launch_rank0, 1):.2f} ms",
             "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz "

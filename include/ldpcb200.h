@@ -91,6 +91,8 @@ typedef struct {
     uint64_t max_iters;    /* largest iteration count of one frame */
     float kernel_ms;       /* device time of the decode kernel (CUDA events on the handle's stream) */
     float reserved1;
+    uint64_t bit_errors_sq; /* sum over frames of (bit errors of the frame)^2: the frame-level variance
+                               of the bit-error count, for confidence intervals on BER */
 } ldpc_tally;
 
 /* Replaces parse_chinn + the device setup of ldpc_sim_scalar.cpp:204-269, 319-392.  Copies the
@@ -126,14 +128,17 @@ int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);
 int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins);
 
 /* Launch shape of the QC kernel's simulation path for one storage mode (-1 = all): rows per thread,
- * frames per CTA, and the resident CTAs per SM its register allocation must allow (a register cap;
- * 0 = the compiler's choice).  All zero restores the default.  LDPC_ENOTSUP if the shape is not
- * built for this code.  Used by the autotuner (ldpcb200.capi.Decoder.autotune). */
+ * frames per CTA, the resident CTAs per SM its register allocation must allow (a register cap;
+ * 0 = the compiler's choice), and whether the check messages live in global memory instead of
+ * registers (1 for codes too large for the register file).  All zero restores the default.
+ * LDPC_ENOTSUP if the shape is not built for this code.  Used by the autotuner
+ * (ldpcb200.capi.Decoder.autotune).  Options with no QC variant built (e.g. clips on a K = 16384
+ * code) run on the general kernel. */
 int ldpc_set_launch_shape(ldpc_handle* h, int storage, int rows_per_thread, int frames_per_cta,
-                          int min_ctas_per_sm);
+                          int min_ctas_per_sm, int global_messages);
 
-/* The QC shapes built for this code and storage mode: writes up to max_shapes triples
- * (rows per thread, frames per CTA, min CTAs per SM) and returns how many exist. */
+/* The QC shapes built for this code and storage mode: writes up to max_shapes quadruples
+ * (rows per thread, frames per CTA, min CTAs per SM, global messages) and returns how many exist. */
 int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes);
 
 /* Number of kernel launches the handle issued since creation (for launch accounting). */

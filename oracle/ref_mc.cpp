@@ -61,7 +61,7 @@ int main(int argc, char** argv) {
     if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
 
     std::atomic<uint64_t> next_pair{0};
-    std::atomic<uint64_t> frames{0}, be{0}, fe{0}, it0{0}, n0{0};
+    std::atomic<uint64_t> frames{0}, be{0}, be2{0}, fe{0}, it0{0}, n0{0};
     const uint64_t max_pairs = (max_frames + 1) / 2;
     const auto t0 = std::chrono::steady_clock::now();
     auto worker = [&]() {
@@ -78,6 +78,7 @@ int main(int argc, char** argv) {
                                  s[0], s[1], s[2], s[3], h.data(), llr.data(), rmsg.data(), st);
             frames += 2;
             be += st[0];
+            be2 += (uint64_t)st[0] * st[0];
             fe += st[1];
             it0 += st[2];
             n0 += 1;
@@ -87,9 +88,9 @@ int main(int argc, char** argv) {
     for (int t = 0; t < threads; t++) pool.emplace_back(worker);
     for (auto& t : pool) t.join();
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    printf("{\"frames\": %llu, \"bit_errors\": %llu, \"frame_errors\": %llu, \"cw0_iter_sum\": %llu, "
-           "\"cw0_count\": %llu, \"elapsed_s\": %.6f, \"threads\": %d}\n",
-           (unsigned long long)frames.load(), (unsigned long long)be.load(),
+    printf("{\"frames\": %llu, \"bit_errors\": %llu, \"bit_errors_sq_pairs\": %llu, \"frame_errors\": %llu, "
+           "\"cw0_iter_sum\": %llu, \"cw0_count\": %llu, \"elapsed_s\": %.6f, \"threads\": %d}\n",
+           (unsigned long long)frames.load(), (unsigned long long)be.load(), (unsigned long long)be2.load(),
            (unsigned long long)fe.load(), (unsigned long long)it0.load(),
            (unsigned long long)n0.load(), el, threads);
     return 0;

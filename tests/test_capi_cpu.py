@@ -33,7 +33,7 @@ def test_struct_layouts():
     # sizes the C side uses (include/ldpcb200.h); a mismatch would corrupt every call
     assert C.sizeof(capi.Matrix) == 24
     assert C.sizeof(capi.RunParams) == 64
-    assert C.sizeof(capi.Tally) == 56
+    assert C.sizeof(capi.Tally) == 64
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

@@ -135,11 +135,11 @@ def test_paired_kernel_matches_oracle(dec_r12k1, storage, n):
     mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.0)
     rng = np.random.default_rng(7 + n)
     llr = (mu + sigma * rng.standard_normal((n, c.n_tx))).astype(np.float32)
-    dec_r12k1.set_launch_shape(1, 2, 0, storage=storage)
+    dec_r12k1.set_launch_shape(1, 2, 0, 0, storage=storage)
     try:
         post, it, sf, be, tal = dec_r12k1.decode_llr(llr, max_iter=60, storage=storage)
     finally:
-        dec_r12k1.set_launch_shape(0, 0, 0, storage=storage)
+        dec_r12k1.set_launch_shape(0, 0, 0, 0, storage=storage)
     mode = {"bf16": O.STORE_BF16, "fp16": O.STORE_FP16}[storage]
     opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=60)
     assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
@@ -149,7 +149,7 @@ def test_paired_kernel_matches_oracle(dec_r12k1, storage, n):
 def test_paired_kernel_on_reference_golden(golden, dec_r12k1):
     """The paired kernel on every fixture case of the reference worker it supports (rate 1/2
     K=1024 in makeH order, Approximate-Min*, no clips): the reference's bits."""
-    dec_r12k1.set_launch_shape(1, 2, 0, storage="bf16")
+    dec_r12k1.set_launch_shape(1, 2, 0, 0, storage="bf16")
     try:
         n = 0
         for case in golden["cases"]:
@@ -161,7 +161,7 @@ def test_paired_kernel_on_reference_golden(golden, dec_r12k1):
             n += 1
         assert n >= 10
     finally:
-        dec_r12k1.set_launch_shape(0, 0, 0, storage="bf16")
+        dec_r12k1.set_launch_shape(0, 0, 0, 0, storage="bf16")
 
 
 @pytest.mark.parametrize("storage", ["bf16", "fp16"])
@@ -171,10 +171,47 @@ def test_paired_sim_path_equals_single(dec_r12k1, storage):
     mu, sigma = capi.channel_mu_sigma(2560, 1536, 512, 1.5)
     p = dec_r12k1.params(mu=mu, sigma=sigma, seed=3, first_frame=77, n_frames=5001, max_iter=200, storage=storage)
     single = dec_r12k1.run_chunk(p)
-    dec_r12k1.set_launch_shape(1, 2, 0, storage=storage)
+    dec_r12k1.set_launch_shape(1, 2, 0, 0, storage=storage)
     try:
         paired = dec_r12k1.run_chunk(p)
     finally:
-        dec_r12k1.set_launch_shape(0, 0, 0, storage=storage)
+        dec_r12k1.set_launch_shape(0, 0, 0, 0, storage=storage)
     for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters"):
         assert getattr(single, k) == getattr(paired, k), k
+
+
+@pytest.mark.parametrize("K,rate", ar4ja.ALL_CODES)
+@pytest.mark.parametrize("storage", ["bf16", "fp16", "fp32"])
+def test_every_ar4ja_code_vs_oracle(gpu, K, rate, storage):
+    """All nine codes through the C ABI (the layered QC kernel; K = 16384 with its messages in
+    global memory; the general kernel where a storage mode is not built for a shape) against the
+    oracle with the same storage: bit for bit."""
+    from ldpcb200 import threshold
+    c = ar4ja.make_code(K, rate)
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db(rate) + 0.8)
+    rng = np.random.default_rng(K + len(rate) + len(storage))
+    n = 3 if K == 16384 else 6
+    llr = (mu + sigma * rng.standard_normal((n, c.n_tx))).astype(np.float32)
+    with capi.Decoder.from_code(c, 0) as dec:
+        assert dec.kind == capi.KERNEL_QC
+        post, it, sf, be, tal = dec.decode_llr(llr, max_iter=25, storage=storage)
+    mode = {"bf16": O.STORE_BF16, "fp32": O.STORE_FP32, "fp16": O.STORE_FP16}[storage]
+    opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=25)
+    assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
+    assert np.array_equal(_bits(post), _bits(opost))
+
+
+def test_options_without_qc_variant_use_general_kernel(gpu):
+    """Min-sum with clips on a K = 16384 code has no QC variant: the general kernel (one frame per
+    CTA for this length) decodes it, bit-exact to the oracle."""
+    c = ar4ja.make_code(16384, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.6)
+    rng = np.random.default_rng(5)
+    llr = (mu + sigma * rng.standard_normal((2, c.n_tx))).astype(np.float32)
+    with capi.Decoder.from_code(c, 0) as dec:
+        post, it, sf, be, tal = dec.decode_llr(llr, max_iter=15, storage="bf16", algo=capi.ALGO_NMS, r_max=6.0,
+                                               l_post_max=40.0)
+    opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=O.STORE_BF16, algo=O.ALGO_NMS,
+                                    max_iter=15, r_max=6.0, l_post_max=40.0)
+    assert np.array_equal(it, oit) and np.array_equal(be, obe)
+    assert np.array_equal(_bits(post), _bits(opost))

@@ -11,25 +11,6 @@
 
 namespace ldpcb200 {
 
-template <int MODE> struct RTraits;
-template <> struct RTraits<STORE_BF16> {
-    using T = uint16_t;
-    static __device__ __forceinline__ float ld(const T* p) { return __uint_as_float(uint32_t(*p) << 16); }
-    static __device__ __forceinline__ void st(T* p, float v) { *p = __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
-};
-template <> struct RTraits<STORE_FP32> {
-    using T = float;
-    static __device__ __forceinline__ float ld(const T* p) { return *p; }
-    static __device__ __forceinline__ void st(T* p, float v) { *p = v; }
-};
-template <> struct RTraits<STORE_FP16> {
-    using T = uint16_t;
-    static __device__ __forceinline__ float ld(const T* p) { return __half2float(__ushort_as_half(*p)); }
-    static __device__ __forceinline__ void st(T* p, float v) {
-        *p = __half_as_ushort(__float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f)));
-    }
-};
-
 // One row of degree deg <= DT, updated by one lane (ldpc_decoder_core.h:414-520).
 template <int DT, int MODE, int ALGO>
 __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTraits<MODE>::T* L,
@@ -98,8 +79,9 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
         }
 }
 
-template <int DT, int MODE, int ALGO, bool EXT>
-__global__ void __launch_bounds__(32 * GEN_WARPS) general_kernel(const __grid_constant__ GenParams p) {
+// NW: frame slots (warps) per CTA; large codes use one so that a slot's L fits shared memory.
+template <int DT, int MODE, int ALGO, bool EXT, int NW = GEN_WARPS>
+__global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant__ GenParams p) {
     using LT = LTraits<MODE>;
     using LE = typename LT::T;
     using RE = typename RTraits<MODE>::T;
@@ -108,11 +90,11 @@ __global__ void __launch_bounds__(32 * GEN_WARPS) general_kernel(const __grid_co
     const int N = p.N, M = p.M;
     const int lstride = (N + 7) & ~7;
     LE* L = reinterpret_cast<LE*>(smem_raw) + (size_t)warp * lstride;
-    const size_t slot = (size_t)blockIdx.x * GEN_WARPS + warp;
+    const size_t slot = (size_t)blockIdx.x * NW + warp;
     RE* r = reinterpret_cast<RE*>(p.r_base) + slot * (size_t)p.dmax * M;
     const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
-    unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0;
+    unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0, t_be2 = 0;
 
     for (;;) {
         uint32_t fid = 0;
@@ -191,6 +173,7 @@ __global__ void __launch_bounds__(32 * GEN_WARPS) general_kernel(const __grid_co
         if (lane == 0) {
             t_frames += 1;
             t_be += be;
+            t_be2 += (unsigned long long)be * be;
             t_fe += be > 0;
             t_it += (unsigned)it;
             t_unc += sfail != 0;
@@ -213,6 +196,7 @@ __global__ void __launch_bounds__(32 * GEN_WARPS) general_kernel(const __grid_co
         atomicAdd(&p.tally[T_ITER_SUM], t_it);
         atomicAdd(&p.tally[T_UNCONVERGED], t_unc);
         atomicMax(&p.tally[T_MAX_ITER], t_max);
+        atomicAdd(&p.tally[T_BIT_ERR_SQ], t_be2);
     }
 }
 
@@ -275,48 +259,53 @@ void free_general(GeneralCode* g) {
     g->r_cap = 0;
 }
 
-template <int DT, int MODE, int ALGO, bool EXT>
+template <int DT, int MODE, int ALGO, bool EXT, int NW = GEN_WARPS>
 static const void* gk() {
-    return reinterpret_cast<const void*>(&general_kernel<DT, MODE, ALGO, EXT>);
+    return reinterpret_cast<const void*>(&general_kernel<DT, MODE, ALGO, EXT, NW>);
 }
 
-template <int DT, int MODE>
+template <int DT, int MODE, int NW = GEN_WARPS>
 static const void* pick_algo(int algo, bool ext) {
-    if (algo == ALGO_AMIN) return ext ? gk<DT, MODE, ALGO_AMIN, true>() : gk<DT, MODE, ALGO_AMIN, false>();
-    return ext ? gk<DT, MODE, ALGO_NMS, true>() : gk<DT, MODE, ALGO_NMS, false>();
+    if (algo == ALGO_AMIN) return ext ? gk<DT, MODE, ALGO_AMIN, true, NW>() : gk<DT, MODE, ALGO_AMIN, false, NW>();
+    return ext ? gk<DT, MODE, ALGO_NMS, true, NW>() : gk<DT, MODE, ALGO_NMS, false, NW>();
 }
 
-template <int DT>
+template <int DT, int NW = GEN_WARPS>
 static const void* pick_mode(int mode, int algo, bool ext) {
-    if (mode == STORE_BF16) return pick_algo<DT, STORE_BF16>(algo, ext);
-    if (mode == STORE_FP32) return pick_algo<DT, STORE_FP32>(algo, ext);
-    return pick_algo<DT, STORE_FP16>(algo, ext);
+    if (mode == STORE_BF16) return pick_algo<DT, STORE_BF16, NW>(algo, ext);
+    if (mode == STORE_FP32) return pick_algo<DT, STORE_FP32, NW>(algo, ext);
+    return pick_algo<DT, STORE_FP16, NW>(algo, ext);
 }
 
 int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                    const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                    unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,
                    int n_sm, cudaStream_t stream, std::string& err) {
-    const void* fn = g->dt == 8    ? pick_mode<8>(p->storage, p->algo, ext)
-                     : g->dt == 20 ? pick_mode<20>(p->storage, p->algo, ext)
-                                   : pick_mode<32>(p->storage, p->algo, ext);
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
-    const size_t smem = (size_t)GEN_WARPS * ((g->N + 7) & ~7) * esz;
+    // four frame slots per CTA while their L arrays fit comfortably in shared memory, else one
+    const int nw = (size_t)GEN_WARPS * ((g->N + 7) & ~7) * esz <= 160 * 1024 ? GEN_WARPS : 1;
+    const void* fn = nw == GEN_WARPS ? (g->dt == 8    ? pick_mode<8>(p->storage, p->algo, ext)
+                                        : g->dt == 20 ? pick_mode<20>(p->storage, p->algo, ext)
+                                                      : pick_mode<32>(p->storage, p->algo, ext))
+                                     : (g->dt == 8    ? pick_mode<8, 1>(p->storage, p->algo, ext)
+                                        : g->dt == 20 ? pick_mode<20, 1>(p->storage, p->algo, ext)
+                                                      : pick_mode<32, 1>(p->storage, p->algo, ext));
+    const size_t smem = (size_t)nw * ((g->N + 7) & ~7) * esz;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return gfail(err, LDPC_ENOTSUP, "general kernel: frame too large for shared memory");
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * GEN_WARPS, smem) != cudaSuccess || per_sm <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * nw, smem) != cudaSuccess || per_sm <= 0) {
         cudaGetLastError();
         return gfail(err, LDPC_ENOTSUP, "general kernel does not fit on an SM");
     }
-    const uint64_t want = (n + GEN_WARPS - 1) / GEN_WARPS;
+    const uint64_t want = (n + nw - 1) / nw;
     const uint64_t grid = std::min<uint64_t>(want, (uint64_t)per_sm * n_sm);
     if (!grid) return 0;
     const size_t rsz = p->storage == STORE_FP32 ? 4 : 2;
-    const size_t need = grid * GEN_WARPS * (size_t)g->dmax * g->M * rsz;
+    const size_t need = grid * nw * (size_t)g->dmax * g->M * rsz;
     if (g->r_cap < need) {
         cudaFree(g->d_r);
         g->d_r = nullptr;
@@ -358,7 +347,7 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
     gp.hist_bins = hist_bins;
     gp.work = d_work;
     void* args[] = {&gp};
-    cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * GEN_WARPS), args, smem, stream);
+    cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * nw), args, smem, stream);
     if (e != cudaSuccess) return gfail(err, LDPC_EIO, std::string("general kernel launch: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -571,6 +560,7 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         out->max_iters = t[T_MAX_ITER];
         out->kernel_ms = 0.0f;
         out->reserved1 = 0.0f;
+        out->bit_errors_sq = t[T_BIT_ERR_SQ];
     }
     return 0;
 }

@@ -69,7 +69,12 @@ struct ldpc_handle {
     int Z = 0, D = 0;
     int32_t blk_off[QC_LAYERS][QC_DMAX] = {};
     int32_t shift[QC_LAYERS][QC_DMAX] = {};
-    int shape[3][3] = {};  // per storage mode: rows per thread, frames per CTA, min CTAs/SM (0 = default)
+    // per storage mode: rows per thread, frames per CTA, min CTAs/SM, messages in global memory;
+    // all zero = the default shape
+    int shape[3][4] = {};
+    void* d_rmsg = nullptr;  // message scratch of RG kernels
+    size_t rmsg_cap = 0;
+    bool gen_built = false;
     // general structure (device)
     GeneralCode gen{};
     // device scratch
@@ -162,6 +167,7 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     cudaFree(h->d_llr);
     cudaFree(h->d_post);
     cudaFree(h->d_frame_out);
+    cudaFree(h->d_rmsg);
     free_general(&h->gen);
     if (h->h_tally) cudaFreeHost(h->h_tally);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -220,6 +226,7 @@ extern "C" int ldpc_create(const ldpc_matrix* m, int device, ldpc_handle** out) 
         h->kind = LDPC_KERNEL_GENERAL;
         if ((rc = build_general(h->rows.data(), h->N, h->M, h->P, h->dmax, &h->gen, g_err)) != 0)
             return bail(rc);
+        h->gen_built = true;
     }
     *out = h;
     return 0;
@@ -237,25 +244,46 @@ extern "C" int64_t ldpc_launch_param_bytes(const ldpc_handle* h) {
     return h->kind == LDPC_KERNEL_QC ? (int64_t)sizeof(QcParams) : (int64_t)sizeof(GenParams);
 }
 
-static bool shape_built(const ldpc_handle* h, int storage, int R, int F, int B) {
-    return find_qc(QcKey{h->Z, h->D, R, F, storage, LDPC_ALGO_AMIN, 0, 0, B}) != nullptr;
+static const void* find_shape(const ldpc_handle* h, int storage, int algo, int clip, int ext, int R, int F, int B, int G) {
+    return find_qc(QcKey{h->Z, h->D, R, F, storage, algo, clip, ext, B, G});
 }
 
-extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B) {
+// The default shape of a numerics variant: one row per thread and one frame per CTA with messages in
+// registers when that is built, else the first shape built for it (e.g. the global-message kernel of
+// a K = 16384 code).
+static bool default_shape(const ldpc_handle* h, int storage, int algo, int clip, int ext, int s[4]) {
+    if (find_shape(h, storage, algo, clip, ext, 1, 1, 0, 0)) {
+        s[0] = 1; s[1] = 1; s[2] = 0; s[3] = 0;
+        return true;
+    }
+    for (const QcTable* t = qc_tables(); t; t = t->next)
+        for (int i = 0; i < t->count; ++i) {
+            const QcKey& k = t->entries[i].key;
+            if (k.Z == h->Z && k.D == h->D && k.mode == storage && k.algo == algo && k.clip == clip && k.ext == ext) {
+                s[0] = k.R; s[1] = k.F; s[2] = k.B; s[3] = k.G;
+                return true;
+            }
+        }
+    return false;
+}
+
+extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0)
-        return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d", storage, R, F, B);
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 1)
+        return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
-    const int r = R ? R : 1, f = F ? F : 1;
-    bool any = false;
-    for (int s = lo; s <= hi; ++s) any |= shape_built(h, s, r, f, B);
-    if (!any) return fail(LDPC_ENOTSUP, "shape R=%d F=%d B=%d not built for Z=%d D=%d", r, f, B, h->Z, h->D);
+    const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
+    bool any = reset;
+    for (int s = lo; s <= hi; ++s) any |= find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) != nullptr;
+    if (!any)
+        return fail(LDPC_ENOTSUP, "shape R=%d F=%d B=%d G=%d not built for Z=%d D=%d", R, F, B, G, h->Z, h->D);
     for (int s = lo; s <= hi; ++s)
-        if (shape_built(h, s, r, f, B) || (R == 0 && F == 0 && B == 0)) {
+        if (reset || find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G)) {
             h->shape[s][0] = R;
             h->shape[s][1] = F;
             h->shape[s][2] = B;
+            h->shape[s][3] = G;
         }
     return 0;
 }
@@ -269,9 +297,10 @@ extern "C" int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shap
             const QcKey& k = t->entries[i].key;
             if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != LDPC_ALGO_AMIN || k.clip || k.ext) continue;
             if (n < max_shapes) {
-                shapes[3 * n] = k.R;
-                shapes[3 * n + 1] = k.F;
-                shapes[3 * n + 2] = k.B;
+                shapes[4 * n] = k.R;
+                shapes[4 * n + 1] = k.F;
+                shapes[4 * n + 2] = k.B;
+                shapes[4 * n + 3] = k.G;
             }
             ++n;
         }
@@ -293,20 +322,18 @@ static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
 static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                      const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
     const bool clip = p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f;
-    int R = h->shape[p->storage][0] ? h->shape[p->storage][0] : 1;
-    int F = h->shape[p->storage][1] ? h->shape[p->storage][1] : 1;
-    QcKey key{h->Z, h->D, R, F, p->storage, p->algo, clip ? 1 : 0, ext ? 1 : 0, h->shape[p->storage][2]};
-    const void* fn = find_qc(key);
-    if (!fn && (R != 1 || F != 1 || key.B != 0)) {  // fall back to the default shape of the same numerics
-        key.R = 1;
-        key.F = 1;
-        key.B = 0;
-        fn = find_qc(key);
-        R = F = 1;
+    int sh[4] = {h->shape[p->storage][0], h->shape[p->storage][1], h->shape[p->storage][2], h->shape[p->storage][3]};
+    const void* fn = nullptr;
+    if (sh[0] || sh[1] || sh[2] || sh[3])
+        fn = find_shape(h, p->storage, p->algo, clip, ext, sh[0] ? sh[0] : 1, sh[1] ? sh[1] : 1, sh[2], sh[3]);
+    if (fn) {
+        sh[0] = sh[0] ? sh[0] : 1;
+        sh[1] = sh[1] ? sh[1] : 1;
+    } else if (default_shape(h, p->storage, p->algo, clip, ext, sh)) {
+        fn = find_shape(h, p->storage, p->algo, clip, ext, sh[0], sh[1], sh[2], sh[3]);
     }
-    if (!fn)
-        return fail(LDPC_ENOTSUP, "QC kernel Z=%d D=%d storage=%d algo=%d clip=%d ext=%d is not built", h->Z,
-                    h->D, p->storage, p->algo, (int)clip, (int)ext);
+    if (!fn) return LDPC_ENOTSUP;  // the caller falls back to the general kernel
+    const int R = sh[0], F = sh[1], G = sh[3];
     QcParams qp;
     memset(&qp, 0, sizeof qp);
     memcpy(qp.blk_off, h->blk_off, sizeof qp.blk_off);
@@ -334,6 +361,12 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
     qp.hist_bins = h->hist_bins;
     qp.work = h->d_work;
     const int T = h->Z / R;
+    int32_t off = 0;
+    for (int l = 0; l < QC_LAYERS; ++l) {
+        qp.layer_off[l] = off;
+        off += h->Z * (l < 4 ? QC_DEG_LOW : h->D);
+    }
+    qp.slot_elems = off;
     const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;
     const size_t lstride = (size_t)((h->N + 7) & ~7);
     const size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
@@ -344,6 +377,12 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
     const uint64_t want = (n + F - 1) / F;
     const uint64_t grid = std::min<uint64_t>(want, (uint64_t)per_sm * h->n_sm);
     if (grid == 0) return 0;
+    if (G) {
+        int rc;
+        const size_t rsz = p->storage == LDPC_STORE_FP32 ? 4 : 2;
+        if ((rc = ensure_cap(&h->d_rmsg, &h->rmsg_cap, grid * F * (size_t)qp.slot_elems * rsz))) return rc;
+        qp.r_base = h->d_rmsg;
+    }
     void* args[] = {&qp};
     CU(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(T), args, smem, h->stream));
     h->launches++;
@@ -372,6 +411,7 @@ static int read_tally(ldpc_handle* h, ldpc_tally* out) {
         out->max_iters = h->h_tally[T_MAX_ITER];
         out->kernel_ms = ms;
         out->reserved1 = 0.0f;
+        out->bit_errors_sq = h->h_tally[T_BIT_ERR_SQ];
     }
     return 0;
 }
@@ -393,13 +433,18 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
         int32_t* it = d_it ? d_it + off : nullptr;
         int32_t* sf = d_sf ? d_sf + off : nullptr;
         int32_t* be = d_be ? d_be + off : nullptr;
-        if (h->kind == LDPC_KERNEL_QC)
-            rc = launch_qc(h, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be);
-        else
+        rc = LDPC_ENOTSUP;
+        if (h->kind == LDPC_KERNEL_QC) rc = launch_qc(h, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be);
+        if (rc == LDPC_ENOTSUP) {  // no QC variant for these options: the general kernel decodes any matrix
+            if (!h->gen_built) {
+                if ((rc = build_general(h->rows.data(), h->N, h->M, h->P, h->dmax, &h->gen, g_err)) != 0) return rc;
+                h->gen_built = true;
+            }
             rc = launch_general(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be, h->d_tally,
                                 h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err);
+            if (!rc) h->launches++;
+        }
         if (rc) return rc;
-        if (h->kind != LDPC_KERNEL_QC) h->launches++;
     }
     CU(cudaEventRecord(h->ev1, h->stream));
     CU(cudaGetLastError());

@@ -53,10 +53,13 @@ struct QcParams {
     unsigned long long* hist;             // [hist_bins] iterations histogram (optional)
     int32_t hist_bins;
     unsigned int* work;                   // frame claim counter, zero at launch
+    void* r_base;                         // messages in global memory (RG kernels): [slot][edges]
+    int32_t layer_off[QC_LAYERS];         // element offset of layer l's messages in a slot ([edge][row])
+    int32_t slot_elems;                   // messages per slot (edges of the code)
 };
 
 enum TallyWord : int {
-    T_FRAMES = 0, T_BIT_ERR, T_FRAME_ERR, T_ITER_SUM, T_UNCONVERGED, T_MAX_ITER, T_CYCLES, TALLY_WORDS = 8
+    T_FRAMES = 0, T_BIT_ERR, T_FRAME_ERR, T_ITER_SUM, T_UNCONVERGED, T_MAX_ITER, T_BIT_ERR_SQ, TALLY_WORDS = 8
 };
 
 template <int MODE> struct LTraits;
@@ -75,6 +78,26 @@ template <> struct LTraits<STORE_FP32> {
     static __device__ __forceinline__ float round_ch(float v) { return v; }
 };
 template <> struct LTraits<STORE_FP16> : LTraits<STORE_FP32> {};
+
+// Check messages as stored in memory (one element per edge), for kernels that keep them there.
+template <int MODE> struct RTraits;
+template <> struct RTraits<STORE_BF16> {
+    using T = uint16_t;
+    static __device__ __forceinline__ float ld(const T* p) { return __uint_as_float(uint32_t(*p) << 16); }
+    static __device__ __forceinline__ void st(T* p, float v) { *p = __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+};
+template <> struct RTraits<STORE_FP32> {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T* p) { return *p; }
+    static __device__ __forceinline__ void st(T* p, float v) { *p = v; }
+};
+template <> struct RTraits<STORE_FP16> {
+    using T = uint16_t;
+    static __device__ __forceinline__ float ld(const T* p) { return __half2float(__ushort_as_half(*p)); }
+    static __device__ __forceinline__ void st(T* p, float v) {
+        *p = __half_as_ushort(__float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f)));
+    }
+};
 
 // Messages of one row in registers.
 template <int d, int MODE> struct RowMsg {  // 16-bit storage: pairs packed in 32-bit words
@@ -116,11 +139,23 @@ template <int d> struct RowMsg<d, STORE_FP32> {
     }
 };
 
+// Messages of one row kept in global memory (RG kernels): edge e at p[e * stride].  A slot's
+// messages are laid out [layer][edge][row], so the threads of a CTA touch consecutive addresses.
+template <int d, int MODE> struct RowMsgGlobal {
+    typename RTraits<MODE>::T* p;
+    int stride;
+    __device__ __forceinline__ float get(int e) const { return RTraits<MODE>::ld(p + (size_t)e * stride); }
+    __device__ __forceinline__ void set2(int e, float a, float b) {
+        RTraits<MODE>::st(p + (size_t)e * stride, a);
+        if (e + 1 < d) RTraits<MODE>::st(p + (size_t)(e + 1) * stride, b);
+    }
+};
+
 // Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
 // sL + f*lstride).  idx[e]: the row's column indices.
-template <int d, int MODE, int ALGO, bool CLIP, int F>
+template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG>
 __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
-                                           RowMsg<d, MODE> (&rm)[F], float r_cap, float lp_cap) {
+                                           MSG (&rm)[F], float r_cap, float lp_cap) {
     using LT = LTraits<MODE>;
     float q[F][d];
 #pragma unroll
@@ -326,8 +361,9 @@ template <int MODE, bool PAIR> struct SlotView {
     __device__ __forceinline__ uint32_t sign(int i) const { return LTraits<MODE>::sign(p, at(i)); }
 };
 
-// Registers holding the messages of one CTA's rows: [layer][row][slot] rows, or one pair per row.
-template <int D, int R, int F, int MODE, bool PAIR> struct MsgRegs {
+// Registers holding the messages of one CTA's rows: [layer][row][slot] rows, or one pair per row,
+// or nothing when the messages live in global memory (RG).
+template <int D, int R, int F, int MODE, bool PAIR, bool RG = false> struct MsgRegs {
     RowMsg<QC_DEG_LOW, MODE> r3[4][R][F];
     RowMsg<D, MODE> rD[8][R][F];
     __device__ __forceinline__ void zero_slot(int f) {
@@ -341,7 +377,10 @@ template <int D, int R, int F, int MODE, bool PAIR> struct MsgRegs {
             for (int rho = 0; rho < R; ++rho) rD[l][rho][f].zero();
     }
 };
-template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, true> {
+template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, false, true> {
+    __device__ __forceinline__ void zero_slot(int) {}
+};
+template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, true, false> {
     RowMsgPair<QC_DEG_LOW, MODE> r3[4];
     RowMsgPair<D, MODE> rD[8];
     __device__ __forceinline__ void zero_slot(int f) {
@@ -355,14 +394,18 @@ template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, true> {
 // B: resident CTAs per SM the register allocation must allow (0 = the compiler's choice); a larger B
 // caps registers per thread at 65536 / (B * Z/R) and trades registers for resident warps.
 // PAIR: the paired mode above (F = 2, R = 1, 16-bit storage, Approximate-Min*, no clips).
-template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false>
+// RG: messages in global memory (p.r_base, one region of p.slot_elems per slot) instead of
+// registers, for codes whose rows per thread times degrees exceed the register file (K = 16384).
+template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false,
+          bool RG = false>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
     static_assert(Z % 32 == 0 && Z % R == 0 && T % 32 == 0, "Z must be a multiple of 32 and of 32*R");
     static_assert(F >= 1 && F <= QC_MAX_F, "frames per CTA");
-    static_assert(!PAIR || (F == 2 && R == 1 && MODE != STORE_FP32 && ALGO == ALGO_AMIN && !CLIP),
+    static_assert(!PAIR || (F == 2 && R == 1 && MODE != STORE_FP32 && ALGO == ALGO_AMIN && !CLIP && !RG),
                   "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
+    using RE = typename RTraits<MODE>::T;
     using SV = SlotView<MODE, PAIR>;
     using LT = LTraits<MODE>;
     using LE = typename LT::T;
@@ -382,7 +425,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
 
-    MsgRegs<D, R, F, MODE, PAIR> msg;
+    MsgRegs<D, R, F, MODE, PAIR, RG> msg;
 
     uint32_t act = 0;                // active slots (uniform)
     uint32_t need = (1u << F) - 1u;  // slots waiting for a frame (uniform)
@@ -392,7 +435,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     for (int f = 0; f < F; ++f) { it[f] = 0; fid[f] = 0xFFFFFFFFu; }
 
     // per-CTA tallies, kept by thread 0
-    unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0;
+    unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0, t_be2 = 0;
 
     for (;;) {
         // ---------------------------------------------------------------- refill
@@ -413,7 +456,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 it[f] = 0;
                 if (fid[f] == 0xFFFFFFFFu) { act &= ~(1u << f); continue; }
                 act |= 1u << f;
-                msg.zero_slot(f);
+                if constexpr (RG) {  // each thread clears exactly the messages of its own rows
+                    RE* rs = reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems;
+                    for (int i = tid; i < p.slot_elems; i += T) rs[i] = RE(0);
+                } else {
+                    msg.zero_slot(f);
+                }
                 const SV L(sL, f, lstride);
                 const int nq = p.n_tx >> 2;
                 if (EXT) {
@@ -466,7 +514,15 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         int idx[QC_DEG_LOW];
 #pragma unroll
                         for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
-                        if constexpr (PAIR)
+                        if constexpr (RG) {
+                            RowMsgGlobal<QC_DEG_LOW, MODE> rm[F];
+#pragma unroll
+                            for (int f = 0; f < F; ++f)
+                                rm[f] = RowMsgGlobal<QC_DEG_LOW, MODE>{
+                                    reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
+                                        p.layer_off[l] + j, Z};
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap);
+                        } else if constexpr (PAIR)
                             row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
                         else
                             row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap);
@@ -474,7 +530,15 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         int idx[D];
 #pragma unroll
                         for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
-                        if constexpr (PAIR)
+                        if constexpr (RG) {
+                            RowMsgGlobal<D, MODE> rm[F];
+#pragma unroll
+                            for (int f = 0; f < F; ++f)
+                                rm[f] = RowMsgGlobal<D, MODE>{
+                                    reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
+                                        p.layer_off[l] + j, Z};
+                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap);
+                        } else if constexpr (PAIR)
                             row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
                         else
                             row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap, lp_cap);
@@ -552,6 +616,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             if (tid == 0) {
                 t_frames += 1;
                 t_be += be;
+            t_be2 += (unsigned long long)be * be;
+                t_be2 += (unsigned long long)be * be;
                 t_fe += be > 0;
                 t_it += (unsigned)it[f];
                 t_unc += sf != 0;
@@ -578,6 +644,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
         atomicAdd(&p.tally[T_ITER_SUM], t_it);
         atomicAdd(&p.tally[T_UNCONVERGED], t_unc);
         atomicMax(&p.tally[T_MAX_ITER], t_max);
+        atomicAdd(&p.tally[T_BIT_ERR_SQ], t_be2);
     }
 }
 

@@ -8,11 +8,12 @@ namespace ldpcb200 {
 
 struct QcKey {
     int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
+    int G;                                     // 1: messages in global memory (RG kernel)
     // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
     // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
         return Z == o.Z && D == o.D && R == o.R && F == o.F && mode == o.mode && algo == o.algo &&
-               clip == o.clip && ext == o.ext && B == o.B;
+               clip == o.clip && ext == o.ext && B == o.B && G == o.G;
     }
 };
 
@@ -35,11 +36,15 @@ const QcTable* qc_tables();
 
 #define LDPC_QC_ENTRY(Z, D, R, F, MODE, ALGO, CLIP, EXT) LDPC_QC_ENTRY_B(Z, D, R, F, MODE, ALGO, CLIP, EXT, 0)
 #define LDPC_QC_ENTRY_B(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                  \
-    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B},                                   \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 0},                                \
      reinterpret_cast<const void*>(&::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B>)}
+#define LDPC_QC_ENTRY_G(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                  \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 1},                                \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true>)}
 
 #define LDPC_QC_ENTRY_PAIR(Z, D, MODE, EXT, B)                                 \
-    {{Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, 0, EXT, B},                     \
+    {{Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, 0, EXT, B, 0},                  \
      reinterpret_cast<const void*>(                                            \
          &::ldpcb200::qc_decode_kernel<Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, false, EXT, B, true>)}
 

@@ -51,7 +51,7 @@ class RunParams(C.Structure):
 class Tally(C.Structure):
     _fields_ = [("frames", C.c_uint64), ("bit_errors", C.c_uint64), ("frame_errors", C.c_uint64),
                 ("iter_sum", C.c_uint64), ("unconverged", C.c_uint64), ("max_iters", C.c_uint64),
-                ("kernel_ms", C.c_float), ("reserved1", C.c_float)]
+                ("kernel_ms", C.c_float), ("reserved1", C.c_float), ("bit_errors_sq", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
@@ -79,7 +79,7 @@ def load(path: str = LIB_PATH):
                                   P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
     L.ldpc_channel_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float)]
     L.ldpc_iter_histogram.argtypes = [C.c_void_p, P(C.c_uint64), C.c_int]
-    L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_launch_count.argtypes = [C.c_void_p]
     L.ldpc_launch_count.restype = C.c_int64
@@ -138,7 +138,7 @@ def decode_llr_static(rows: np.ndarray, n_vars: int, n_punct: int, p: RunParams,
                                       d_iters or None, d_synd_fail or None, d_bit_errors or None, C.byref(t),
                                       stream or None))
     return ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
-                       t.kernel_ms)
+                       t.kernel_ms, t.bit_errors_sq)
 
 
 @dataclass
@@ -150,6 +150,7 @@ class ChunkResult:
     unconverged: int
     max_iters: int
     kernel_ms: float
+    bit_errors_sq: int = 0
 
 
 class Decoder:
@@ -202,18 +203,20 @@ class Decoder:
         return _check(int(self._lib.ldpc_launch_param_bytes(self._h)))
 
     def set_launch_shape(self, rows_per_thread: int = 0, frames_per_cta: int = 0, min_ctas_per_sm: int = 0,
-                         storage=-1):
+                         global_messages: int = 0, storage=-1):
         if isinstance(storage, str):
             storage = STORAGE_NAMES[storage]
-        _check(self._lib.ldpc_set_launch_shape(self._h, storage, rows_per_thread, frames_per_cta, min_ctas_per_sm))
+        _check(self._lib.ldpc_set_launch_shape(self._h, storage, rows_per_thread, frames_per_cta, min_ctas_per_sm,
+                                               global_messages))
 
     def shapes(self, storage) -> list:
-        """Built QC launch shapes (rows per thread, frames per CTA, min CTAs per SM) for a storage mode."""
+        """Built QC launch shapes (rows per thread, frames per CTA, min CTAs per SM, global messages)
+        for a storage mode."""
         if isinstance(storage, str):
             storage = STORAGE_NAMES[storage]
-        buf = np.zeros(3 * 64, np.int32)
+        buf = np.zeros(4 * 64, np.int32)
         n = _check(self._lib.ldpc_list_shapes(self._h, storage, _ip(buf), 64))
-        return [tuple(int(x) for x in buf[3 * i:3 * i + 3]) for i in range(min(n, 64))]
+        return [tuple(int(x) for x in buf[4 * i:4 * i + 4]) for i in range(min(n, 64))]
 
     def autotune(self, mu: float, sigma: float, storages=("fp32", "fp16", "bf16"), frames: int = 1 << 18,
                  max_iter: int = 200, seed: int = 0x5EED, repeats: int = 2):
@@ -251,7 +254,7 @@ class Decoder:
         t = Tally()
         _check(self._lib.ldpc_run_chunk(self._h, C.byref(p), C.byref(t)))
         return ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged,
-                           t.max_iters, t.kernel_ms)
+                           t.max_iters, t.kernel_ms, t.bit_errors_sq)
 
     def decode_llr(self, llr: np.ndarray, p: Optional[RunParams] = None, want_post: bool = True, **kw):
         """Decode caller-supplied channel LLRs [n, N-P].  Returns (post [n, N] or None, iters,
@@ -270,7 +273,7 @@ class Decoder:
         _check(self._lib.ldpc_decode_llr(self._h, C.byref(p), _fp(llr), n, _fp(post), _ip(it), _ip(sf),
                                          _ip(be), C.byref(t)))
         return post, it, sf, be, ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum,
-                                             t.unconverged, t.max_iters, t.kernel_ms)
+                                             t.unconverged, t.max_iters, t.kernel_ms, t.bit_errors_sq)
 
     def channel_llr(self, p: RunParams) -> np.ndarray:
         out = np.empty((int(p.n_frames), self.n_tx), np.float32)

@@ -29,5 +29,22 @@ def poisson_interval(k: int, conf: float = 0.95) -> Tuple[float, float]:
     return lo, hi
 
 
+def ber_interval(bit_errors: int, bit_errors_sq: int, units: int, bits_per_unit: int,
+                 conf: float = 0.95) -> Tuple[float, float]:
+    """Interval for BER that respects error clustering: the independent unit is the frame (or the
+    codeword pair), not the bit, because a failed frame carries hundreds of correlated bit errors.
+    Normal interval on the mean bit-error count per unit from its sample variance (sum of squares);
+    with no errors at all, the Clopper-Pearson bound on units with an error, times the unit's bits."""
+    if units <= 1:
+        return 0.0, 1.0
+    z = float(_st.norm.ppf(0.5 + conf / 2))
+    if bit_errors == 0:
+        return 0.0, clopper_pearson(0, units, conf)[1]
+    mean = bit_errors / units
+    var = max(bit_errors_sq / units - mean * mean, 0.0) * units / (units - 1)
+    half = z * (var / units) ** 0.5
+    return max(0.0, mean - half) / bits_per_unit, (mean + half) / bits_per_unit
+
+
 def intervals_overlap(a: Tuple[float, float], b: Tuple[float, float]) -> bool:
     return a[0] <= b[1] and b[0] <= a[1]
