@@ -78,7 +78,12 @@ typedef struct {
     float l_max;        /* channel LLR clip (-L / -G), 0 = off  (ldpc_decoder_core.h:266-275) */
     float r_max;        /* check message clip (-R), 0 = off      (:487) */
     float l_post_max;   /* posterior clip (-V), 0 = off          (:492-495) */
+    float ebn0_lo_db;   /* per-frame Eb/N0: when ebn0_hi_db > ebn0_lo_db every frame draws its Eb/N0 */
+    float ebn0_hi_db;   /* uniformly in [lo, hi) from its own counter, and mu/sigma are ignored */
 } ldpc_run_params;
+
+/* Bins of the per-frame Eb/N0 range (ldpc_snr_bins). */
+#define LDPC_SNR_BINS 32
 
 /* Tallies of one call: the per-worker stats of run_ldpc_worker (ldpc_decoder_core.h:580-585)
  * summed over all frames of the chunk. */
@@ -127,6 +132,11 @@ int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);
  * iterations (the last bin also counts every larger value). */
 int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins);
 
+/* Per-Eb/N0 tallies of the last ldpc_run_chunk with a per-frame Eb/N0 range: out[k * LDPC_SNR_BINS + b]
+ * for k = frames, frame errors, bit errors, iterations, and bin b of [lo, hi) in LDPC_SNR_BINS equal
+ * steps. */
+int ldpc_snr_bins(ldpc_handle* h, uint64_t* out);
+
 /* Launch shape of the QC kernel's simulation path for one storage mode (-1 = all): rows per thread,
  * frames per CTA, the resident CTAs per SM its register allocation must allow (a register cap;
  * 0 = the compiler's choice), and whether the check messages live in global memory instead of
@@ -170,6 +180,23 @@ int64_t ldpc_launch_param_bytes(const ldpc_handle* h);
 int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr,
                            int64_t n_frames, float* d_post, int32_t* d_iters, int32_t* d_synd_fail,
                            int32_t* d_bit_errors, ldpc_tally* out, void* stream);
+
+/* A batch of codes on one device decoded by one CUDA graph launch (the mixed-code workload).  The
+ * reference runs one code per process (run_simulation.py:164-193); this has no counterpart there.
+ * Every handle must have the QC structure. */
+typedef struct ldpc_batch ldpc_batch;
+int ldpc_batch_create(ldpc_handle* const* handles, int n_handles, ldpc_batch** out);
+void ldpc_batch_destroy(ldpc_batch* b);
+
+/* One graph launch: per handle i, params[i] (n_frames may be 0; at most 2^31) decoded by its
+ * persistent kernel.  The kernels have no dependencies on one another.  With share NULL each gets its
+ * full persistent grid and the hardware block scheduler starts a code's CTAs as the CTAs launched
+ * before it retire; otherwise kernel i is limited to the fraction share[i] / sum(share) of the
+ * GPU's CTA slots and the codes run side by side.
+ * out[i] receives handle i's tallies (kernel_ms = the whole graph's device time), *graph_ms the
+ * device time of the launch.  ldpc_snr_bins(handle i) then gives its per-Eb/N0 tallies. */
+int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, const float* share, ldpc_tally* out,
+                   float* graph_ms);
 
 /* Copies the last error message of the calling thread into buf (NUL-terminated); returns its
  * length. */

@@ -32,7 +32,7 @@ def test_library_exports_every_symbol():
 def test_struct_layouts():
     # sizes the C side uses (include/ldpcb200.h); a mismatch would corrupt every call
     assert C.sizeof(capi.Matrix) == 24
-    assert C.sizeof(capi.RunParams) == 64
+    assert C.sizeof(capi.RunParams) == 72
     assert C.sizeof(capi.Tally) == 64
 
 

@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
         if (lane == 0) fid = atomicAdd(p.work, 1u);
         fid = __shfl_sync(0xFFFFFFFFu, fid, 0);
         if (fid >= p.n_frames) break;
+        const bool per_frame_snr = !EXT && p.ebn0_hi > p.ebn0_lo;
+        int snr_bin = 0;
         // channel
         if (EXT) {
             const float* src = p.llr_in + (size_t)fid * p.n_tx;
@@ -111,9 +113,12 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
             }
         } else {
             const uint64_t gf = p.first_frame + fid;
+            float ch_mu = p.mu, ch_sigma = p.sigma;
+            if (per_frame_snr)
+                frame_snr(p.ebn0_lo, p.ebn0_hi, p.rate, gf, p.stream, p.seed_lo, p.seed_hi, ch_mu, ch_sigma, snr_bin);
             for (int qd = lane; qd * 4 < p.n_tx; qd += 32) {
                 float n[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                if (p.sigma > 0.0f) {
+                if (ch_sigma > 0.0f) {
                     const U32x4 x = philox4x32_10(U32x4{(uint32_t)qd, (uint32_t)gf, (uint32_t)(gf >> 32), p.stream},
                                                   p.seed_lo, p.seed_hi);
                     box_muller(x.x, x.y, n[0], n[1]);
@@ -122,7 +127,7 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (4 * qd + k >= p.n_tx) break;
-                    float x = p.sigma > 0.0f ? __fmaf_rn(p.sigma, n[k], p.mu) : p.mu;
+                    float x = ch_sigma > 0.0f ? __fmaf_rn(ch_sigma, n[k], ch_mu) : ch_mu;
                     if (p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
                     LT::st(L, 4 * qd + k, x);
                 }
@@ -179,6 +184,12 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
             t_unc += sfail != 0;
             t_max = max(t_max, (unsigned long long)it);
             if (p.hist) atomicAdd(&p.hist[min(it, p.hist_bins - 1)], 1ull);
+            if (per_frame_snr && p.snr_bins) {
+                atomicAdd(&p.snr_bins[snr_bin], 1ull);
+                atomicAdd(&p.snr_bins[SNR_BINS + snr_bin], (unsigned long long)(be > 0));
+                atomicAdd(&p.snr_bins[2 * SNR_BINS + snr_bin], (unsigned long long)be);
+                atomicAdd(&p.snr_bins[3 * SNR_BINS + snr_bin], (unsigned long long)it);
+            }
             if (p.iters_out) p.iters_out[fid] = it;
             if (p.synd_out) p.synd_out[fid] = (int32_t)sfail;
             if (p.be_out) p.be_out[fid] = (int32_t)be;
@@ -280,7 +291,7 @@ static const void* pick_mode(int mode, int algo, bool ext) {
 int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                    const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                    unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,
-                   int n_sm, cudaStream_t stream, std::string& err) {
+                   int n_sm, cudaStream_t stream, std::string& err, unsigned long long* d_snr_bins) {
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
     // four frame slots per CTA while their L arrays fit comfortably in shared memory, else one
     const int nw = (size_t)GEN_WARPS * ((g->N + 7) & ~7) * esz <= 160 * 1024 ? GEN_WARPS : 1;
@@ -346,6 +357,10 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
     gp.hist = d_hist;
     gp.hist_bins = hist_bins;
     gp.work = d_work;
+    gp.ebn0_lo = p->ebn0_lo_db;
+    gp.ebn0_hi = p->ebn0_hi_db;
+    gp.rate = (float)((double)(g->N - g->M) / (double)(g->N - g->P));
+    gp.snr_bins = d_snr_bins;
     void* args[] = {&gp};
     cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * nw), args, smem, stream);
     if (e != cudaSuccess) return gfail(err, LDPC_EIO, std::string("general kernel launch: ") + cudaGetErrorString(e));

@@ -82,6 +82,7 @@ struct ldpc_handle {
     unsigned int* d_work = nullptr;
     unsigned long long* d_hist = nullptr;
     int hist_bins = 0;
+    unsigned long long* d_snr = nullptr;  // [4][SNR_BINS]
     float* d_llr = nullptr;
     size_t llr_cap = 0;
     float* d_post = nullptr;
@@ -164,6 +165,7 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     cudaFree(h->d_tally);
     cudaFree(h->d_work);
     cudaFree(h->d_hist);
+    cudaFree(h->d_snr);
     cudaFree(h->d_llr);
     cudaFree(h->d_post);
     cudaFree(h->d_frame_out);
@@ -218,7 +220,8 @@ extern "C" int ldpc_create(const ldpc_matrix* m, int device, ldpc_handle** out) 
         cudaMallocHost(&h->h_tally, TALLY_WORDS * sizeof(unsigned long long)) != cudaSuccess)
         return bail(fail(LDPC_ENOMEM, "device allocation failed"));
     h->hist_bins = 1024;
-    if (cudaMalloc(&h->d_hist, h->hist_bins * sizeof(unsigned long long)) != cudaSuccess)
+    if (cudaMalloc(&h->d_hist, h->hist_bins * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&h->d_snr, 4 * SNR_BINS * sizeof(unsigned long long)) != cudaSuccess)
         return bail(fail(LDPC_ENOMEM, "device allocation failed"));
     if (detect_qc(h) && h->N - h->P > 0 && ((h->N - h->P) % 32) == 0) {
         h->kind = LDPC_KERNEL_QC;
@@ -316,11 +319,27 @@ static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
     if (!(p->l_max >= 0.0f) || !(p->r_max >= 0.0f) || !(p->l_post_max >= 0.0f))
         return fail(LDPC_EINVAL, "clips must be >= 0");
     if (!(p->sigma >= 0.0f) || p->mu != p->mu) return fail(LDPC_EINVAL, "bad channel mu/sigma");
+    if (!(p->ebn0_lo_db > -100.0f && p->ebn0_lo_db < 100.0f) || !(p->ebn0_hi_db > -100.0f && p->ebn0_hi_db < 100.0f))
+        return fail(LDPC_EINVAL, "per-frame Eb/N0 range must lie in (-100, 100) dB");
     return 0;
 }
 
-static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
-                     const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
+// A prepared QC launch: kernel, grid, block, dynamic shared memory and its parameter block.
+struct QcLaunch {
+    const void* fn = nullptr;
+    unsigned grid = 0;
+    int block = 0;
+    size_t smem = 0;
+    QcParams qp;
+};
+
+static double code_rate(const ldpc_handle* h) { return (double)(h->N - h->M) / (double)(h->N - h->P); }
+
+// Chooses the QC kernel for these numerics and shape and fills its launch; grid_frac < 1 gives the
+// launch that share of the GPU's resident CTA slots (for kernels that run side by side).
+static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
+                      const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
+                      double grid_frac, QcLaunch* out) {
     const bool clip = p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f;
     int sh[4] = {h->shape[p->storage][0], h->shape[p->storage][1], h->shape[p->storage][2], h->shape[p->storage][3]};
     const void* fn = nullptr;
@@ -334,7 +353,7 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
     }
     if (!fn) return LDPC_ENOTSUP;  // the caller falls back to the general kernel
     const int R = sh[0], F = sh[1], G = sh[3];
-    QcParams qp;
+    QcParams& qp = out->qp;
     memset(&qp, 0, sizeof qp);
     memcpy(qp.blk_off, h->blk_off, sizeof qp.blk_off);
     memcpy(qp.shift, h->shift, sizeof qp.shift);
@@ -360,6 +379,10 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
     qp.hist = h->d_hist;
     qp.hist_bins = h->hist_bins;
     qp.work = h->d_work;
+    qp.ebn0_lo = p->ebn0_lo_db;
+    qp.ebn0_hi = p->ebn0_hi_db;
+    qp.rate = (float)code_rate(h);
+    qp.snr_bins = h->d_snr;
     const int T = h->Z / R;
     int32_t off = 0;
     for (int l = 0; l < QC_LAYERS; ++l) {
@@ -375,7 +398,12 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
     if (per_sm <= 0) return fail(LDPC_ENOTSUP, "QC kernel does not fit on an SM (smem %zu)", smem);
     const uint64_t want = (n + F - 1) / F;
-    const uint64_t grid = std::min<uint64_t>(want, (uint64_t)per_sm * h->n_sm);
+    const uint64_t cap = std::max<uint64_t>(1, (uint64_t)((double)per_sm * h->n_sm * std::min(1.0, grid_frac) + 0.5));
+    const uint64_t grid = std::min<uint64_t>(want, cap);
+    out->fn = fn;
+    out->grid = (unsigned)grid;
+    out->block = T;
+    out->smem = smem;
     if (grid == 0) return 0;
     if (G) {
         int rc;
@@ -383,8 +411,16 @@ static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_
         if ((rc = ensure_cap(&h->d_rmsg, &h->rmsg_cap, grid * F * (size_t)qp.slot_elems * rsz))) return rc;
         qp.r_base = h->d_rmsg;
     }
-    void* args[] = {&qp};
-    CU(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(T), args, smem, h->stream));
+    return 0;
+}
+
+static int launch_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
+                     const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
+    QcLaunch L;
+    int rc = prepare_qc(h, p, ext, n, first, d_llr, d_post, d_it, d_sf, d_be, 1.0, &L);
+    if (rc || L.grid == 0) return rc;
+    void* args[] = {&L.qp};
+    CU(cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.block), args, L.smem, h->stream));
     h->launches++;
     return 0;
 }
@@ -393,6 +429,7 @@ static int reset_counters(ldpc_handle* h) {
     CU(cudaMemsetAsync(h->d_tally, 0, TALLY_WORDS * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(h->d_work, 0, 64, h->stream));
     CU(cudaMemsetAsync(h->d_hist, 0, h->hist_bins * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(h->d_snr, 0, 4 * SNR_BINS * sizeof(unsigned long long), h->stream));
     return 0;
 }
 
@@ -441,7 +478,7 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
                 h->gen_built = true;
             }
             rc = launch_general(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be, h->d_tally,
-                                h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err);
+                                h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err, h->d_snr);
             if (!rc) h->launches++;
         }
         if (rc) return rc;
@@ -493,13 +530,16 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
 
 // Channel only: the Philox/Box-Muller LLRs of a range of frames, for checking the generator.
 __global__ void channel_kernel(float* out, int ntx, uint64_t first, uint64_t n, uint32_t seed_lo, uint32_t seed_hi,
-                               uint32_t stream, float mu, float sigma) {
+                               uint32_t stream, float mu0, float sigma0, float lo, float hi, float rate) {
     const int nq = ntx >> 2;
     const uint64_t total = n * (uint64_t)nq;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t f = i / nq;
         const int qd = (int)(i % nq);
         const uint64_t gf = first + f;
+        float mu = mu0, sigma = sigma0;
+        int bin;
+        if (hi > lo) frame_snr(lo, hi, rate, gf, stream, seed_lo, seed_hi, mu, sigma, bin);
         float v[4];
         if (sigma > 0.0f) {
             const U32x4 x = philox4x32_10(U32x4{(uint32_t)qd, (uint32_t)gf, (uint32_t)(gf >> 32), stream}, seed_lo, seed_hi);
@@ -524,7 +564,8 @@ extern "C" int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float*
     if (!bytes) return 0;
     if ((rc = ensure_cap((void**)&h->d_llr, &h->llr_cap, bytes))) return rc;
     channel_kernel<<<h->n_sm * 8, 256, 0, h->stream>>>(h->d_llr, ntx, p->first_frame, p->n_frames, (uint32_t)p->seed,
-                                                       (uint32_t)(p->seed >> 32), p->stream, p->mu, p->sigma);
+                                                       (uint32_t)(p->seed >> 32), p->stream, p->mu, p->sigma,
+                                                       p->ebn0_lo_db, p->ebn0_hi_db, (float)code_rate(h));
     h->launches++;
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(llr, h->d_llr, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -548,5 +589,162 @@ extern "C" int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins) {
     CU(cudaStreamSynchronize(h->stream));
     for (int i = 0; i < n_bins; ++i) hist[i] = 0;
     for (int i = 0; i < h->hist_bins; ++i) hist[std::min(i, n_bins - 1)] += tmp[i];
+    return 0;
+}
+
+extern "C" int ldpc_snr_bins(ldpc_handle* h, uint64_t* out) {
+    if (!h || !out) return fail(LDPC_EINVAL, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    unsigned long long tmp[4 * SNR_BINS];
+    CU(cudaMemcpyAsync(tmp, h->d_snr, sizeof tmp, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < 4 * SNR_BINS; ++i) out[i] = tmp[i];
+    return 0;
+}
+
+// ----------------------------------------------------------------------------- batched launch
+// Several codes decoded by one CUDA graph launch: per code, memset nodes for its counters followed by
+// its persistent kernel; the codes' kernels have no dependencies on one another and run side by
+// side, each on its share of the GPU's CTA slots, each claiming frames from its own queue.
+struct ldpc_batch {
+    int device = 0;
+    std::vector<ldpc_handle*> hs;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int64_t launches = 0;
+};
+
+extern "C" int ldpc_batch_create(ldpc_handle* const* handles, int n, ldpc_batch** out) {
+    if (!out || !handles || n <= 0) return fail(LDPC_EINVAL, "bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!handles[i]) return fail(LDPC_EINVAL, "handle %d is NULL", i);
+        if (handles[i]->device != handles[0]->device) return fail(LDPC_EINVAL, "handles on different devices");
+        if (handles[i]->kind != LDPC_KERNEL_QC)
+            return fail(LDPC_ENOTSUP, "handle %d does not have the QC structure (batches take QC codes)", i);
+    }
+    ldpc_batch* b = new (std::nothrow) ldpc_batch();
+    if (!b) return fail(LDPC_ENOMEM, "host allocation failed");
+    b->device = handles[0]->device;
+    b->hs.assign(handles, handles + n);
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
+        cudaGetLastError();
+        ldpc_batch_destroy(b);
+        return fail(LDPC_EIO, "stream/event creation failed");
+    }
+    *out = b;
+    return 0;
+}
+
+extern "C" void ldpc_batch_destroy(ldpc_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+static int add_memset(cudaGraph_t g, void* dst, size_t bytes, cudaGraphNode_t* node) {
+    cudaMemsetParams mp = {};
+    mp.dst = dst;
+    mp.value = 0;
+    mp.elementSize = 4;
+    mp.width = bytes / 4;
+    mp.height = 1;
+    mp.pitch = 0;
+    CU(cudaGraphAddMemsetNode(node, g, nullptr, 0, &mp));
+    return 0;
+}
+
+extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, const float* share, ldpc_tally* out,
+                              float* graph_ms) {
+    if (!b || !params) return fail(LDPC_EINVAL, "bad arguments");
+    CU(cudaSetDevice(b->device));
+    const int n = (int)b->hs.size();
+    double work_total = 0.0;
+    std::vector<double> w(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        int rc;
+        if ((rc = check_params(b->hs[i], &params[i]))) return rc;
+        if (params[i].n_frames > kMaxLaunchFrames) return fail(LDPC_EINVAL, "code %d: at most 2^31 frames per batch", i);
+        w[i] = share ? (double)share[i] : 1.0;
+        if (!(w[i] >= 0.0)) return fail(LDPC_EINVAL, "share %d is negative", i);
+        work_total += params[i].n_frames ? w[i] : 0.0;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CU(cudaGraphCreate(&g, 0));
+    int rc = 0;
+    int64_t kernels = 0;
+    for (int i = 0; i < n && !rc; ++i) {
+        ldpc_handle* h = b->hs[i];
+        cudaGraphNode_t deps[4];
+        if ((rc = add_memset(g, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), &deps[0])) ||
+            (rc = add_memset(g, h->d_work, 64, &deps[1])) ||
+            (rc = add_memset(g, h->d_hist, h->hist_bins * sizeof(unsigned long long), &deps[2])) ||
+            (rc = add_memset(g, h->d_snr, 4 * SNR_BINS * sizeof(unsigned long long), &deps[3])))
+            break;
+        if (!params[i].n_frames) continue;
+        QcLaunch L;
+        // no shares: every kernel gets its full persistent grid and the block scheduler starts the
+        // next code's CTAs as the previous code's retire
+        const double frac = (share && work_total > 0.0) ? w[i] / work_total : 1.0;
+        rc = prepare_qc(h, &params[i], false, (uint32_t)params[i].n_frames, params[i].first_frame, nullptr, nullptr,
+                        nullptr, nullptr, nullptr, frac, &L);
+        if (rc == LDPC_ENOTSUP) {
+            rc = fail(LDPC_ENOTSUP, "code %d: no QC kernel for these options", i);
+            break;
+        }
+        if (rc || !L.grid) continue;
+        void* args[] = {&L.qp};
+        cudaKernelNodeParams kp = {};
+        kp.func = const_cast<void*>(L.fn);
+        kp.gridDim = dim3(L.grid);
+        kp.blockDim = dim3(L.block);
+        kp.sharedMemBytes = (unsigned)L.smem;
+        kp.kernelParams = args;
+        cudaGraphNode_t kn;
+        const cudaError_t e = cudaGraphAddKernelNode(&kn, g, deps, 4, &kp);
+        if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphAddKernelNode: %s", cudaGetErrorString(e));
+        ++kernels;
+    }
+    if (!rc) {
+        const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
+        cudaError_t e = cudaEventRecord(b->e0, b->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ge, b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->e1, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) rc = fail(LDPC_EIO, "graph launch: %s", cudaGetErrorString(e));
+    }
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    if (rc) return rc;
+    b->launches += kernels;
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, b->e0, b->e1));
+    if (graph_ms) *graph_ms = ms;
+    for (int i = 0; i < n; ++i) {
+        ldpc_handle* h = b->hs[i];
+        h->launches += params[i].n_frames ? 1 : 0;
+        unsigned long long t[TALLY_WORDS];
+        CU(cudaMemcpy(t, h->d_tally, sizeof t, cudaMemcpyDeviceToHost));
+        if (out) {
+            out[i].frames = t[T_FRAMES];
+            out[i].bit_errors = t[T_BIT_ERR];
+            out[i].frame_errors = t[T_FRAME_ERR];
+            out[i].iter_sum = t[T_ITER_SUM];
+            out[i].unconverged = t[T_UNCONVERGED];
+            out[i].max_iters = t[T_MAX_ITER];
+            out[i].kernel_ms = ms;
+            out[i].reserved1 = 0.0f;
+            out[i].bit_errors_sq = t[T_BIT_ERR_SQ];
+        }
+    }
     return 0;
 }

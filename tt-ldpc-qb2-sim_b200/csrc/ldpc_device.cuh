@@ -46,6 +46,21 @@ __device__ __forceinline__ void box_muller(uint32_t x0, uint32_t x1, float& n0, 
     n1 = rad * s;
 }
 
+// Per-frame Eb/N0 for mixed workloads: uniform in [lo, hi) dB, drawn from the frame's Philox stream
+// with counter word 0 = 0xFFFFFFFF (the channel uses words 0 .. N/4), then the LLR mean and deviation
+// of that Eb/N0 at code rate R (mu = 4 R Eb/N0, sigma = sqrt(8 R Eb/N0)) and its bin of [lo, hi).
+constexpr int SNR_BINS = 32;
+
+__device__ __forceinline__ void frame_snr(float lo, float hi, float rate, uint64_t frame, uint32_t stream,
+                                          uint32_t k0, uint32_t k1, float& mu, float& sigma, int& bin) {
+    const U32x4 x = philox4x32_10(U32x4{0xFFFFFFFFu, (uint32_t)frame, (uint32_t)(frame >> 32), stream}, k0, k1);
+    const float u = __uint2float_rz(x.x >> 8) * (1.0f / 16777216.0f);
+    const float g = exp10f(0.1f * __fmaf_rn(hi - lo, u, lo));
+    mu = 4.0f * rate * g;
+    sigma = sqrtf(8.0f * rate * g);
+    bin = min((int)(u * (float)SNR_BINS), SNR_BINS - 1);
+}
+
 // ------------------------------------------------------------------ storage rounding
 __device__ __forceinline__ float bf16_round(float x) {  // fp32_to_bf16, RNE (ldpc_decoder_core.h:84-90)
     return __bfloat162float(__float2bfloat16_rn(x));

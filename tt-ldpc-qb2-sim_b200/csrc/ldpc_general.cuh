@@ -46,6 +46,8 @@ struct GenParams {
     unsigned long long* hist;
     int32_t hist_bins;
     unsigned int* work;
+    float ebn0_lo, ebn0_hi, rate;         // per-frame Eb/N0 (see QcParams)
+    unsigned long long* snr_bins;
 };
 
 int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCode* g, std::string& err);
@@ -57,6 +59,6 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
 int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                    const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                    unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,
-                   int n_sm, cudaStream_t stream, std::string& err);
+                   int n_sm, cudaStream_t stream, std::string& err, unsigned long long* d_snr_bins = nullptr);
 
 }  // namespace ldpcb200

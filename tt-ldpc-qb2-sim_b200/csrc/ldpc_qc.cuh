@@ -56,6 +56,9 @@ struct QcParams {
     void* r_base;                         // messages in global memory (RG kernels): [slot][edges]
     int32_t layer_off[QC_LAYERS];         // element offset of layer l's messages in a slot ([edge][row])
     int32_t slot_elems;                   // messages per slot (edges of the code)
+    float ebn0_lo, ebn0_hi;               // per-frame Eb/N0 range in dB (used when hi > lo)
+    float rate;                           // (N - M) / (N - P), for the per-frame mu and sigma
+    unsigned long long* snr_bins;         // [4][SNR_BINS]: frames, frame errors, bit errors, iterations
 };
 
 enum TallyWord : int {
@@ -431,8 +434,10 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     uint32_t need = (1u << F) - 1u;  // slots waiting for a frame (uniform)
     int it[F];
     uint32_t fid[F];
+    int snr_bin[F];
 #pragma unroll
-    for (int f = 0; f < F; ++f) { it[f] = 0; fid[f] = 0xFFFFFFFFu; }
+    for (int f = 0; f < F; ++f) { it[f] = 0; fid[f] = 0xFFFFFFFFu; snr_bin[f] = 0; }
+    const bool per_frame_snr = !EXT && p.ebn0_hi > p.ebn0_lo;
 
     // per-CTA tallies, kept by thread 0
     unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0, t_be2 = 0;
@@ -478,9 +483,13 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                     }
                 } else {
                     const uint64_t gf = p.first_frame + fid[f];
+                    float ch_mu = p.mu, ch_sigma = p.sigma;
+                    if (per_frame_snr)
+                        frame_snr(p.ebn0_lo, p.ebn0_hi, p.rate, gf, p.stream, p.seed_lo, p.seed_hi, ch_mu, ch_sigma,
+                                  snr_bin[f]);
                     for (int qd = tid; qd < nq; qd += T) {
                         float n[4];
-                        if (p.sigma > 0.0f) {
+                        if (ch_sigma > 0.0f) {
                             const U32x4 x = philox4x32_10(U32x4{(uint32_t)qd, (uint32_t)gf, (uint32_t)(gf >> 32), p.stream},
                                                           p.seed_lo, p.seed_hi);
                             box_muller(x.x, x.y, n[0], n[1]);
@@ -490,7 +499,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         }
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            float x = p.sigma > 0.0f ? __fmaf_rn(p.sigma, n[k], p.mu) : p.mu;
+                            float x = ch_sigma > 0.0f ? __fmaf_rn(ch_sigma, n[k], ch_mu) : ch_mu;
                             if (CLIP && p.l_max > 0.0f) x = fminf(fmaxf(x, -p.l_max), p.l_max);
                             L.st(4 * qd + k, x);
                         }
@@ -623,6 +632,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 t_unc += sf != 0;
                 t_max = max(t_max, (unsigned long long)it[f]);
                 if (p.hist) atomicAdd(&p.hist[min(it[f], p.hist_bins - 1)], 1ull);
+                if (per_frame_snr && p.snr_bins) {
+                    atomicAdd(&p.snr_bins[snr_bin[f]], 1ull);
+                    atomicAdd(&p.snr_bins[SNR_BINS + snr_bin[f]], (unsigned long long)(be > 0));
+                    atomicAdd(&p.snr_bins[2 * SNR_BINS + snr_bin[f]], (unsigned long long)be);
+                    atomicAdd(&p.snr_bins[3 * SNR_BINS + snr_bin[f]], (unsigned long long)it[f]);
+                }
                 if (p.iters_out) p.iters_out[fid[f]] = it[f];
                 if (p.synd_out) p.synd_out[fid[f]] = (int32_t)sf;
                 if (p.be_out) p.be_out[fid[f]] = (int32_t)be;

@@ -22,7 +22,8 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
-           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_set_launch_shape", "ldpc_list_shapes", "ldpc_launch_count",
+           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_snr_bins", "ldpc_set_launch_shape", "ldpc_list_shapes",
+           "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
 
 
@@ -45,7 +46,11 @@ class RunParams(C.Structure):
     _fields_ = [("mu", C.c_float), ("sigma", C.c_float), ("seed", C.c_uint64), ("stream", C.c_uint32),
                 ("reserved0", C.c_uint32), ("first_frame", C.c_uint64), ("n_frames", C.c_uint64),
                 ("max_iter", C.c_int32), ("storage", C.c_int32), ("algo", C.c_int32),
-                ("l_max", C.c_float), ("r_max", C.c_float), ("l_post_max", C.c_float)]
+                ("l_max", C.c_float), ("r_max", C.c_float), ("l_post_max", C.c_float),
+                ("ebn0_lo_db", C.c_float), ("ebn0_hi_db", C.c_float)]
+
+
+SNR_BINS = 32
 
 
 class Tally(C.Structure):
@@ -79,6 +84,11 @@ def load(path: str = LIB_PATH):
                                   P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
     L.ldpc_channel_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float)]
     L.ldpc_iter_histogram.argtypes = [C.c_void_p, P(C.c_uint64), C.c_int]
+    L.ldpc_snr_bins.argtypes = [C.c_void_p, P(C.c_uint64)]
+    L.ldpc_batch_create.argtypes = [P(C.c_void_p), C.c_int, P(C.c_void_p)]
+    L.ldpc_batch_destroy.argtypes = [C.c_void_p]
+    L.ldpc_batch_destroy.restype = None
+    L.ldpc_batch_run.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), P(Tally), P(C.c_float)]
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_launch_count.argtypes = [C.c_void_p]
@@ -244,11 +254,19 @@ class Decoder:
 
     @staticmethod
     def params(mu=0.0, sigma=0.0, seed=1, stream=0, first_frame=0, n_frames=0, max_iter=200,
-               storage=STORE_BF16, algo=ALGO_AMIN, l_max=0.0, r_max=0.0, l_post_max=0.0) -> RunParams:
+               storage=STORE_BF16, algo=ALGO_AMIN, l_max=0.0, r_max=0.0, l_post_max=0.0,
+               ebn0_lo=0.0, ebn0_hi=0.0) -> RunParams:
+        """Run parameters; ebn0_hi > ebn0_lo draws each frame's Eb/N0 uniformly in [lo, hi) dB."""
         if isinstance(storage, str):
             storage = STORAGE_NAMES[storage]
         return RunParams(mu, sigma, seed, stream, 0, first_frame, n_frames, max_iter, storage, algo,
-                         l_max, r_max, l_post_max)
+                         l_max, r_max, l_post_max, ebn0_lo, ebn0_hi)
+
+    def snr_bins(self) -> np.ndarray:
+        """[4, SNR_BINS] frames, frame errors, bit errors, iterations per Eb/N0 bin of the last run."""
+        out = np.zeros(4 * SNR_BINS, np.uint64)
+        _check(self._lib.ldpc_snr_bins(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out.reshape(4, SNR_BINS)
 
     def run_chunk(self, p: RunParams) -> ChunkResult:
         t = Tally()
@@ -284,3 +302,40 @@ class Decoder:
         h = np.zeros(n_bins, np.uint64)
         _check(self._lib.ldpc_iter_histogram(self._h, h.ctypes.data_as(C.POINTER(C.c_uint64)), n_bins))
         return h
+
+
+class Batch:
+    """Several decoders (codes) on one GPU run by one CUDA graph launch, their persistent kernels side
+    by side (ldpc_batch_* in include/ldpcb200.h)."""
+
+    def __init__(self, decoders):
+        self._lib = load()
+        self.decoders = list(decoders)
+        arr = (C.c_void_p * len(self.decoders))(*[d._h for d in self.decoders])
+        b = C.c_void_p()
+        _check(self._lib.ldpc_batch_create(arr, len(self.decoders), C.byref(b)))
+        self._b = b
+
+    def run(self, params, share=None):
+        """params: one RunParams per decoder; share: relative CTA shares (None = frames x checks).
+        Returns (list of ChunkResult, graph milliseconds)."""
+        n = len(self.decoders)
+        P = (RunParams * n)(*params)
+        T = (Tally * n)()
+        S = (C.c_float * n)(*share) if share is not None else None
+        ms = C.c_float()
+        _check(self._lib.ldpc_batch_run(self._b, P, S, T, C.byref(ms)))
+        res = [ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
+                           t.kernel_ms, t.bit_errors_sq) for t in T]
+        return res, ms.value
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.ldpc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
