@@ -9,6 +9,10 @@ every point the 95% Clopper-Pearson intervals of FER overlap, and so do the 95% 
 Bit errors cluster (a failed frame carries hundreds), so the BER interval takes the frame (GPU) or
 the codeword pair (reference worker) as its independent unit, with the per-unit variance from the
 tallied sums of squared bit-error counts (ldpcb200.stats.ber_interval).
+
+fp32 message storage is a different, more precise decoder than the reference's bf16 one: its FER
+intervals must still overlap the reference's, and its BER must not be worse (its interval's lower
+end at most the reference interval's upper end); in the waterfall it is measurably better.
 """
 import json
 import os
@@ -52,4 +56,7 @@ def test_fer_ber_within_reference_confidence_intervals(golden, gpu, which, stora
             assert intervals_overlap(fer_g, fer_r), (pt["ebn0"], r.frame_errors, pt["frame_errors"])
             ber_g = ber_interval(r.bit_errors, r.bit_errors_sq, r.frames, ntx)
             ber_r = ber_interval(pt["bit_errors"], pt["bit_errors_sq_pairs"], pt["frames"] // 2, 2 * ntx)
-            assert intervals_overlap(ber_g, ber_r), (pt["ebn0"], r.bit_errors, pt["bit_errors"])
+            if storage == "bf16":
+                assert intervals_overlap(ber_g, ber_r), (pt["ebn0"], r.bit_errors, pt["bit_errors"])
+            else:
+                assert ber_g[0] <= ber_r[1], (pt["ebn0"], r.bit_errors, pt["bit_errors"])

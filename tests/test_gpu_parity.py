@@ -19,6 +19,15 @@ def _bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
 
 
+def _check_tally(tal, it, sf, be):
+    """The kernel's in-kernel tallies against its own per-frame outputs."""
+    b = be.astype(np.int64)
+    assert tal.frames == len(be)
+    assert tal.bit_errors == int(b.sum()) and tal.bit_errors_sq == int((b * b).sum())
+    assert tal.frame_errors == int((b > 0).sum()) and tal.unconverged == int((sf != 0).sum())
+    assert tal.iter_sum == int(it.sum()) and tal.max_iters == int(it.max(initial=0))
+
+
 @pytest.fixture(scope="module")
 def dec_r12k1(gpu):
     c = ar4ja.make_code(1024, "1/2")
@@ -60,9 +69,7 @@ def test_golden_reference_worker(golden, idx, gpu):
         assert int(st[0]) == int(be[k].sum())
         assert int(st[1]) == int((be[k] > 0).sum())
         assert int(st[2]) == int(it[2 * p])
-    assert tal.frames == len(frames)
-    assert tal.bit_errors == int(be.sum()) and tal.frame_errors == int((be > 0).sum())
-    assert tal.iter_sum == int(it.sum())
+    _check_tally(tal, it, sf, be)
 
 
 @pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
@@ -144,6 +151,7 @@ def test_paired_kernel_matches_oracle(dec_r12k1, storage, n):
     opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=60)
     assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
     assert np.array_equal(_bits(post), _bits(opost))
+    _check_tally(tal, it, sf, be)
 
 
 def test_paired_kernel_on_reference_golden(golden, dec_r12k1):
@@ -199,6 +207,7 @@ def test_every_ar4ja_code_vs_oracle(gpu, K, rate, storage):
     opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=25)
     assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
     assert np.array_equal(_bits(post), _bits(opost))
+    _check_tally(tal, it, sf, be)
 
 
 def test_options_without_qc_variant_use_general_kernel(gpu):
@@ -215,3 +224,4 @@ def test_options_without_qc_variant_use_general_kernel(gpu):
                                     max_iter=15, r_max=6.0, l_post_max=40.0)
     assert np.array_equal(it, oit) and np.array_equal(be, obe)
     assert np.array_equal(_bits(post), _bits(opost))
+    _check_tally(tal, it, sf, be)

@@ -625,7 +625,6 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             if (tid == 0) {
                 t_frames += 1;
                 t_be += be;
-            t_be2 += (unsigned long long)be * be;
                 t_be2 += (unsigned long long)be * be;
                 t_fe += be > 0;
                 t_it += (unsigned)it[f];
