@@ -43,6 +43,7 @@ extern "C" {
 /* Check-node rule (ldpc_decoder_core.h:320-475; the reference's -n flag selects NMS). */
 #define LDPC_ALGO_AMIN 0 /* Approximate-Min* (Jones, MILCOM 2003) */
 #define LDPC_ALGO_NMS 1  /* normalised min-sum, alpha = 0.75 */
+#define LDPC_ALGO_WAMIN 2 /* weighted Approximate-Min* with the handle's weights (ldpc_set_weights) */
 
 /* Decoder family chosen for a matrix (ldpc_kernel_kind). */
 #define LDPC_KERNEL_QC 0      /* quasi-cyclic layered kernel (AR4JA structure detected) */
@@ -128,6 +129,11 @@ int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, 
  * (before storage rounding): llr [n_frames][N-P] (host).  For checking the channel. */
 int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);
 
+/* As ldpc_channel_llr into a caller-owned device array d_llr [n_frames][N-P] (16-byte aligned),
+ * queued on the stream (NULL: the legacy default stream) without waiting: training frames for the
+ * weighted decoder come from the simulator's own channel.  No counterpart in the reference. */
+int ldpc_channel_llr_device(ldpc_handle* h, const ldpc_run_params* p, float* d_llr, void* stream);
+
 /* Iteration histogram of the last ldpc_run_chunk / ldpc_decode_llr: hist[i] = frames that used i
  * iterations (the last bin also counts every larger value). */
 int ldpc_iter_histogram(ldpc_handle* h, uint64_t* hist, int n_bins);
@@ -150,6 +156,9 @@ int ldpc_set_launch_shape(ldpc_handle* h, int storage, int rows_per_thread, int 
 /* The QC shapes built for this code and storage mode: writes up to max_shapes quadruples
  * (rows per thread, frames per CTA, min CTAs per SM, global messages) and returns how many exist. */
 int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes);
+
+/* As ldpc_list_shapes for the simulation variants of one algorithm (LDPC_ALGO_*). */
+int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo, int32_t* shapes, int max_shapes);
 
 /* Number of kernel launches the handle issued since creation (for launch accounting). */
 int64_t ldpc_launch_count(const ldpc_handle* h);
@@ -180,6 +189,46 @@ int64_t ldpc_launch_param_bytes(const ldpc_handle* h);
 int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr,
                            int64_t n_frames, float* d_post, int32_t* d_iters, int32_t* d_synd_fail,
                            int32_t* d_bit_errors, ldpc_tally* out, void* stream);
+
+/* Weights of the weighted Approximate-Min* decoder for LDPC_ALGO_WAMIN runs of this handle (host
+ * arrays, copied): alpha/beta [n_iter][n_classes] (iteration t >= n_iter uses row n_iter - 1) and
+ * edge_class [12][18], the class of edge e of layer l.  The check-node output becomes
+ * sign * max(alpha[t][c] * m - beta[t][c], 0) in the simulation kernels (with syndrome stop and
+ * tallies, like every other algorithm).  n_iter = 0 removes the weights.  QC codes only; no clips.
+ * No counterpart in the reference. */
+int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float* beta, int n_iter, int n_classes,
+                     const int32_t* edge_class);
+
+/* ---- Weighted Approximate-Min* decoder (training path; no counterpart in the reference) ----
+ * Layered decoding of the handle's QC code for exactly n_iter iterations (no early stop) with
+ * r_e = sign_e * relu(alpha[t][c] * m_e - beta[t][c]): m_e the Approximate-Min* magnitude of edge e,
+ * t the iteration, c = edge_class[l][e] the protograph edge class of edge e of layer l.  The real
+ * type is float (fp64 = 0; alpha = 1, beta = 0 then reproduces the plain fp32 decoder bit for bit)
+ * or double (fp64 = 1, for checking the adjoint against finite differences; rate 1/2 and 4/5 at
+ * K = 1024 only): every array argument below is of that type.  All pointers are device memory owned
+ * by the caller; the workspace holds the activation checkpoints between the forward and the
+ * backward call of the same frames.  Work is queued on the stream; the calls do not wait for it. */
+typedef struct {
+    int32_t n_iter;              /* T, 1..64 */
+    int32_t n_classes;           /* C, 1..64 */
+    int32_t ckpt_every;          /* iterations between activation checkpoints, 1..T */
+    int32_t post_all;            /* 1: posteriors after every iteration [T][n][N]; 0: after the last [1][n][N] */
+    int32_t fp64;                /* 0: float arrays; 1: double arrays */
+    int32_t reserved0;
+    int32_t edge_class[12][18];  /* class of edge e of layer l */
+} ldpc_wdec_config;
+
+int64_t ldpc_wdec_workspace_bytes(const ldpc_handle* h, const ldpc_wdec_config* c, int64_t n_frames);
+
+/* d_llr [n][N-P] channel LLRs, d_alpha/d_beta [T][C] -> d_post (see post_all). */
+int ldpc_wdec_forward(ldpc_handle* h, const ldpc_wdec_config* c, const void* d_llr, int64_t n_frames,
+                      const void* d_alpha, const void* d_beta, void* d_post, void* d_workspace, void* stream);
+
+/* Adjoint of the last forward with this workspace: d_grad_post (shaped like d_post) in; gradients
+ * of alpha and beta ([T][C], overwritten) and of the channel LLRs ([n][N-P], may be NULL) out. */
+int ldpc_wdec_backward(ldpc_handle* h, const ldpc_wdec_config* c, int64_t n_frames, const void* d_alpha,
+                       const void* d_beta, const void* d_grad_post, void* d_grad_alpha, void* d_grad_beta,
+                       void* d_grad_llr, void* d_workspace, void* stream);
 
 /* A batch of codes on one device decoded by one CUDA graph launch (the mixed-code workload).  The
  * reference runs one code per process (run_simulation.py:164-193); this has no counterpart there.

@@ -119,10 +119,10 @@ static int syndrome_failures(int M, int dmax, const int32_t* rows, const int32_t
  *          *bit_errors (sign bits over the first N-P positions).
  * Returns 0, or -1 on bad arguments.
  */
-int oracle_decode(int N, int M, int P, int dmax, const int32_t* rows, const int32_t* degs,
-                  int mode, int algo, int max_iter, float l_max, float r_max, float l_post_max,
-                  const float* llr_tx, float* post, float* r_work, int32_t* iters,
-                  int32_t* synd_fail, int32_t* bit_errors) {
+static int decode_impl(int N, int M, int P, int dmax, const int32_t* rows, const int32_t* degs,
+                       int mode, int algo, int max_iter, float l_max, float r_max, float l_post_max,
+                       const float* llr_tx, float* post, float* r_work, int32_t* iters,
+                       int32_t* synd_fail, int32_t* bit_errors, int early_stop) {
     if (N <= 0 || M <= 0 || P < 0 || P > N || dmax <= 0 || dmax > ORC_MAX_DEG) return -1;
     const int ntx = N - P;
     float* L = post;
@@ -195,7 +195,7 @@ int oracle_decode(int N, int M, int P, int dmax, const int32_t* rows, const int3
                 rm[d] = store_r(mode, rn);
             }
         }
-        if (it >= 2 && syndrome_failures(M, dmax, rows, degs, L) == 0) {
+        if (early_stop && it >= 2 && syndrome_failures(M, dmax, rows, degs, L) == 0) {
             done = 1;
             it_used = it + 1;
             break;
@@ -208,6 +208,26 @@ int oracle_decode(int N, int M, int P, int dmax, const int32_t* rows, const int3
     for (int i = 0; i < ntx; i++) be += (int)(f2u(L[i]) >> 31);
     *bit_errors = be;
     return 0;
+}
+
+int oracle_decode(int N, int M, int P, int dmax, const int32_t* rows, const int32_t* degs,
+                  int mode, int algo, int max_iter, float l_max, float r_max, float l_post_max,
+                  const float* llr_tx, float* post, float* r_work, int32_t* iters,
+                  int32_t* synd_fail, int32_t* bit_errors) {
+    return decode_impl(N, M, P, dmax, rows, degs, mode, algo, max_iter, l_max, r_max, l_post_max, llr_tx,
+                       post, r_work, iters, synd_fail, bit_errors, 1);
+}
+
+/* The same decoder run for exactly max_iter iterations with no syndrome stop: the unrolled decoder
+ * the weighted (trainable) decoder reduces to at unit scale and zero offset.  The reference always
+ * stops early (ldpc_decoder_core.h, the iteration loop's syndrome test); this variant exists to
+ * check that reduction. */
+int oracle_decode_nostop(int N, int M, int P, int dmax, const int32_t* rows, const int32_t* degs,
+                         int mode, int algo, int max_iter, float l_max, float r_max, float l_post_max,
+                         const float* llr_tx, float* post, float* r_work, int32_t* iters,
+                         int32_t* synd_fail, int32_t* bit_errors) {
+    return decode_impl(N, M, P, dmax, rows, degs, mode, algo, max_iter, l_max, r_max, l_post_max, llr_tx,
+                       post, r_work, iters, synd_fail, bit_errors, 0);
 }
 
 /* ---------------- the reference's channel: xoshiro128+ and the polar method ---------------- */

@@ -45,6 +45,8 @@ def lib():
                                     P(C.c_float), P(C.c_float), P(C.c_float),
                                     P(C.c_int32), P(C.c_int32), P(C.c_int32)]
         L.oracle_decode.restype = C.c_int
+        L.oracle_decode_nostop.argtypes = L.oracle_decode.argtypes
+        L.oracle_decode_nostop.restype = C.c_int
         L.oracle_ref_channel_pair.argtypes = [P(C.c_uint32), C.c_float, C.c_float, C.c_int,
                                               P(C.c_float), P(C.c_float)]
         L.oracle_xo_jump.argtypes = [P(C.c_uint32), C.c_int, C.c_int]
@@ -84,10 +86,12 @@ class Code:
 
 
 def decode(code: Code, llr: np.ndarray, mode: int = STORE_BF16, algo: int = ALGO_AMIN,
-           max_iter: int = 200, l_max: float = 0.0, r_max: float = 0.0, l_post_max: float = 0.0):
+           max_iter: int = 200, l_max: float = 0.0, r_max: float = 0.0, l_post_max: float = 0.0,
+           early_stop: bool = True):
     """Decode frames (rows of ``llr`` [n, N-P] fp32).  Returns (post [n, N] f32, iters, synd_fail,
-    bit_errors) as numpy arrays."""
+    bit_errors) as numpy arrays.  early_stop=False runs exactly max_iter iterations."""
     L = lib()
+    fn = L.oracle_decode if early_stop else L.oracle_decode_nostop
     llr = np.ascontiguousarray(np.atleast_2d(llr), dtype=np.float32)
     n = llr.shape[0]
     post = np.zeros((n, code.N), dtype=np.float32)
@@ -97,10 +101,10 @@ def decode(code: Code, llr: np.ndarray, mode: int = STORE_BF16, algo: int = ALGO
     be = np.zeros(n, np.int32)
     for i in range(n):
         it, s, b = C.c_int32(), C.c_int32(), C.c_int32()
-        rc = L.oracle_decode(code.N, code.M, code.P, code.dmax, _p(code.rows, C.c_int32),
-                             _p(code.degs, C.c_int32), mode, algo, max_iter, l_max, r_max, l_post_max,
-                             _p(llr[i], C.c_float), _p(post[i], C.c_float), _p(rw, C.c_float),
-                             C.byref(it), C.byref(s), C.byref(b))
+        rc = fn(code.N, code.M, code.P, code.dmax, _p(code.rows, C.c_int32),
+                _p(code.degs, C.c_int32), mode, algo, max_iter, l_max, r_max, l_post_max,
+                _p(llr[i], C.c_float), _p(post[i], C.c_float), _p(rw, C.c_float),
+                C.byref(it), C.byref(s), C.byref(b))
         if rc != 0:
             raise ValueError("oracle_decode rejected its arguments")
         iters[i], sf[i], be[i] = it.value, s.value, b.value

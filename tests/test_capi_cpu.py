@@ -34,6 +34,7 @@ def test_struct_layouts():
     assert C.sizeof(capi.Matrix) == 24
     assert C.sizeof(capi.RunParams) == 72
     assert C.sizeof(capi.Tally) == 64
+    assert C.sizeof(capi.WdecConfig) == 6 * 4 + 12 * 18 * 4
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

@@ -16,6 +16,7 @@
 #include "ldpc_general.cuh"
 #include "ldpc_qc.cuh"
 #include "ldpc_registry.h"
+#include "ldpc_weighted.cuh"
 
 using namespace ldpcb200;
 
@@ -89,6 +90,10 @@ struct ldpc_handle {
     size_t post_cap = 0;
     int32_t* d_frame_out = nullptr;  // 3 * cap
     size_t frame_cap = 0;
+    // weights of LDPC_ALGO_WAMIN runs
+    float2* d_wtab = nullptr;  // [w_iters][w_classes] (alpha, beta)
+    int w_iters = 0, w_classes = 0;
+    int8_t w_class[QC_LAYERS][QC_DMAX] = {};
     unsigned long long* h_tally = nullptr;  // pinned
     int64_t launches = 0;
 };
@@ -170,6 +175,7 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     cudaFree(h->d_post);
     cudaFree(h->d_frame_out);
     cudaFree(h->d_rmsg);
+    cudaFree(h->d_wtab);
     free_general(&h->gen);
     if (h->h_tally) cudaFreeHost(h->h_tally);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -270,6 +276,44 @@ static bool default_shape(const ldpc_handle* h, int storage, int algo, int clip,
     return false;
 }
 
+extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float* beta, int n_iter, int n_classes,
+                                const int32_t* edge_class) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    if (n_iter == 0) {
+        h->w_iters = 0;
+        return 0;
+    }
+    if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
+    if (!alpha || !beta || !edge_class || n_iter < 0 || n_iter > 1000 || n_classes < 1 || n_classes > 127)
+        return fail(LDPC_EINVAL, "bad weights (n_iter %d, n_classes %d)", n_iter, n_classes);
+    int8_t cls[QC_LAYERS][QC_DMAX] = {};
+    for (int l = 0; l < QC_LAYERS; ++l)
+        for (int e = 0; e < QC_DMAX; ++e) {
+            const int32_t c = edge_class[l * QC_DMAX + e];
+            const bool used = e < (l < 4 ? QC_DEG_LOW : h->D);
+            if (used && (c < 0 || c >= n_classes))
+                return fail(LDPC_EINVAL, "edge class of layer %d edge %d out of range", l, e);
+            cls[l][e] = used ? (int8_t)c : 0;
+        }
+    const size_t cnt = (size_t)n_iter * n_classes;
+    if (cnt * sizeof(float2) > 64 * 1024) return fail(LDPC_EINVAL, "weight table above 64 KB");
+    std::vector<float2> tab(cnt);
+    for (size_t i = 0; i < cnt; ++i) {
+        if (!(alpha[i] == alpha[i]) || !(beta[i] == beta[i])) return fail(LDPC_EINVAL, "NaN weight");
+        tab[i] = make_float2(alpha[i], beta[i]);
+    }
+    CU(cudaSetDevice(h->device));
+    cudaFree(h->d_wtab);
+    h->d_wtab = nullptr;
+    h->w_iters = 0;
+    CU(cudaMalloc(&h->d_wtab, cnt * sizeof(float2)));
+    CU(cudaMemcpy(h->d_wtab, tab.data(), cnt * sizeof(float2), cudaMemcpyHostToDevice));
+    memcpy(h->w_class, cls, sizeof cls);
+    h->w_iters = n_iter;
+    h->w_classes = n_classes;
+    return 0;
+}
+
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
@@ -278,11 +322,14 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
     bool any = reset;
-    for (int s = lo; s <= hi; ++s) any |= find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) != nullptr;
+    auto built = [&](int s) {
+        return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G);
+    };
+    for (int s = lo; s <= hi; ++s) any |= built(s);
     if (!any)
         return fail(LDPC_ENOTSUP, "shape R=%d F=%d B=%d G=%d not built for Z=%d D=%d", R, F, B, G, h->Z, h->D);
     for (int s = lo; s <= hi; ++s)
-        if (reset || find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G)) {
+        if (reset || built(s)) {
             h->shape[s][0] = R;
             h->shape[s][1] = F;
             h->shape[s][2] = B;
@@ -291,14 +338,15 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
     return 0;
 }
 
-extern "C" int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes) {
-    if (!h || storage < 0 || storage > 2 || (max_shapes > 0 && !shapes)) return fail(LDPC_EINVAL, "bad arguments");
+extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo, int32_t* shapes, int max_shapes) {
+    if (!h || storage < 0 || storage > 2 || algo < 0 || algo > 2 || (max_shapes > 0 && !shapes))
+        return fail(LDPC_EINVAL, "bad arguments");
     if (h->kind != LDPC_KERNEL_QC) return 0;
     int n = 0;
     for (const QcTable* t = qc_tables(); t; t = t->next)
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
-            if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != LDPC_ALGO_AMIN || k.clip || k.ext) continue;
+            if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != algo || k.clip || k.ext) continue;
             if (n < max_shapes) {
                 shapes[4 * n] = k.R;
                 shapes[4 * n + 1] = k.F;
@@ -310,12 +358,22 @@ extern "C" int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shap
     return n;
 }
 
+extern "C" int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes) {
+    return ldpc_list_shapes_algo(h, storage, LDPC_ALGO_AMIN, shapes, max_shapes);
+}
+
 static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (!p) return fail(LDPC_EINVAL, "params are NULL");
     if (p->max_iter < 0 || p->max_iter > 1000000) return fail(LDPC_EINVAL, "max_iter %d out of range", p->max_iter);
     if (p->storage < 0 || p->storage > 2) return fail(LDPC_EINVAL, "unknown storage mode %d", p->storage);
-    if (p->algo < 0 || p->algo > 1) return fail(LDPC_EINVAL, "unknown algorithm %d", p->algo);
+    if (p->algo < 0 || p->algo > 2) return fail(LDPC_EINVAL, "unknown algorithm %d", p->algo);
+    if (p->algo == LDPC_ALGO_WAMIN) {
+        if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
+        if (h->w_iters <= 0) return fail(LDPC_EINVAL, "weighted decoding without weights (ldpc_set_weights)");
+        if (p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f)
+            return fail(LDPC_ENOTSUP, "the weighted decoder takes no clips");
+    }
     if (!(p->l_max >= 0.0f) || !(p->r_max >= 0.0f) || !(p->l_post_max >= 0.0f))
         return fail(LDPC_EINVAL, "clips must be >= 0");
     if (!(p->sigma >= 0.0f) || p->mu != p->mu) return fail(LDPC_EINVAL, "bad channel mu/sigma");
@@ -383,6 +441,12 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     qp.ebn0_hi = p->ebn0_hi_db;
     qp.rate = (float)code_rate(h);
     qp.snr_bins = h->d_snr;
+    if (p->algo == LDPC_ALGO_WAMIN) {
+        qp.wtab = h->d_wtab;
+        qp.w_iters = h->w_iters;
+        qp.w_classes = h->w_classes;
+        memcpy(qp.w_class, h->w_class, sizeof qp.w_class);
+    }
     const int T = h->Z / R;
     int32_t off = 0;
     for (int l = 0; l < QC_LAYERS; ++l) {
@@ -392,7 +456,8 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     qp.slot_elems = off;
     const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;
     const size_t lstride = (size_t)((h->N + 7) & ~7);
-    const size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
+    size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
+    if (p->algo == LDPC_ALGO_WAMIN) smem = ((smem + 15) & ~(size_t)15) + (size_t)h->w_iters * h->w_classes * sizeof(float2);
     if (smem > 48 * 1024) CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
@@ -472,6 +537,9 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
         int32_t* be = d_be ? d_be + off : nullptr;
         rc = LDPC_ENOTSUP;
         if (h->kind == LDPC_KERNEL_QC) rc = launch_qc(h, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be);
+        if (rc == LDPC_ENOTSUP && p->algo == LDPC_ALGO_WAMIN)
+            return fail(LDPC_ENOTSUP, "the weighted decoder is not built for Z=%d D=%d with storage %d", h->Z, h->D,
+                        p->storage);
         if (rc == LDPC_ENOTSUP) {  // no QC variant for these options: the general kernel decodes any matrix
             if (!h->gen_built) {
                 if ((rc = build_general(h->rows.data(), h->N, h->M, h->P, h->dmax, &h->gen, g_err)) != 0) return rc;
@@ -570,6 +638,23 @@ extern "C" int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float*
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(llr, h->d_llr, bytes, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+extern "C" int ldpc_channel_llr_device(ldpc_handle* h, const ldpc_run_params* p, float* d_llr, void* stream) {
+    int rc;
+    if ((rc = check_params(h, p))) return rc;
+    if (!d_llr && p->n_frames) return fail(LDPC_EINVAL, "d_llr is NULL");
+    if (!p->n_frames) return 0;
+    const int ntx = h->N - h->P;
+    if (ntx % 4) return fail(LDPC_ENOTSUP, "channel export needs N-P divisible by 4");
+    if (reinterpret_cast<uintptr_t>(d_llr) % 16) return fail(LDPC_EINVAL, "d_llr must be 16-byte aligned");
+    CU(cudaSetDevice(h->device));
+    channel_kernel<<<h->n_sm * 8, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        d_llr, ntx, p->first_frame, p->n_frames, (uint32_t)p->seed, (uint32_t)(p->seed >> 32), p->stream, p->mu,
+        p->sigma, p->ebn0_lo_db, p->ebn0_hi_db, (float)code_rate(h));
+    h->launches++;
+    CU(cudaGetLastError());
     return 0;
 }
 
@@ -746,5 +831,114 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
             out[i].bit_errors_sq = t[T_BIT_ERR_SQ];
         }
     }
+    return 0;
+}
+
+// ----------------------------------------------------------------------------- weighted decoder (training)
+struct WLayout {
+    size_t ckpt, rwork, stash, gr, total;  // offsets (elements of the real type) and total bytes
+};
+
+static int wcheck(const ldpc_handle* h, const ldpc_wdec_config* c, int64_t n, WLayout* lay) {
+    if (!h || !c) return fail(LDPC_EINVAL, "handle or config is NULL");
+    if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
+    const int rb = c->fp64 ? 8 : 4;
+    if (!weighted_supported(h->Z, h->D, rb))
+        return fail(LDPC_ENOTSUP, "the %s weighted decoder is not built for Z=%d D=%d", c->fp64 ? "double" : "float",
+                    h->Z, h->D);
+    if (c->n_iter < 1 || c->n_iter > W_MAX_ITER || c->n_classes < 1 || c->n_classes > W_MAX_CLASSES ||
+        c->ckpt_every < 1 || c->ckpt_every > c->n_iter || n < 0 || n > (1 << 24))
+        return fail(LDPC_EINVAL, "bad weighted-decoder configuration");
+    for (int l = 0; l < QC_LAYERS; ++l)
+        for (int e = 0; e < (l < 4 ? QC_DEG_LOW : h->D); ++e)
+            if (c->edge_class[l][e] < 0 || c->edge_class[l][e] >= c->n_classes)
+                return fail(LDPC_EINVAL, "edge class of layer %d edge %d out of range", l, e);
+    const size_t E = (size_t)h->Z * (4 * QC_DEG_LOW + 8 * h->D);
+    const size_t n_ckpt = (c->n_iter + c->ckpt_every - 1) / c->ckpt_every;
+    lay->ckpt = 0;
+    lay->rwork = lay->ckpt + n_ckpt * n * (h->N + E);
+    lay->stash = lay->rwork + n * E;
+    lay->gr = lay->stash + (size_t)n * c->ckpt_every * E;
+    lay->total = (lay->gr + n * E) * rb;
+    return 0;
+}
+
+static void wparams_fill(const ldpc_handle* h, const ldpc_wdec_config* c, int64_t n, WParams* p) {
+    memset(p, 0, sizeof *p);
+    memcpy(p->blk_off, h->blk_off, sizeof p->blk_off);
+    memcpy(p->shift, h->shift, sizeof p->shift);
+    memcpy(p->edge_class, c->edge_class, sizeof p->edge_class);
+    int32_t off = 0;
+    for (int l = 0; l < QC_LAYERS; ++l) {
+        p->layer_off[l] = off;
+        off += h->Z * (l < 4 ? QC_DEG_LOW : h->D);
+    }
+    p->n_vars = h->N;
+    p->n_tx = h->N - h->P;
+    p->n_edges = off;
+    p->n_iter = c->n_iter;
+    p->n_classes = c->n_classes;
+    p->ckpt_every = c->ckpt_every;
+    p->post_all = c->post_all ? 1 : 0;
+    p->n_frames = (int32_t)n;
+}
+
+extern "C" int64_t ldpc_wdec_workspace_bytes(const ldpc_handle* h, const ldpc_wdec_config* c, int64_t n) {
+    WLayout lay;
+    int rc = wcheck(h, c, n, &lay);
+    return rc ? rc : (int64_t)lay.total;
+}
+
+extern "C" int ldpc_wdec_forward(ldpc_handle* h, const ldpc_wdec_config* c, const void* d_llr, int64_t n,
+                                 const void* d_alpha, const void* d_beta, void* d_post, void* d_ws, void* stream) {
+    WLayout lay;
+    int rc;
+    if ((rc = wcheck(h, c, n, &lay))) return rc;
+    if (n && (!d_llr || !d_alpha || !d_beta || !d_post || !d_ws)) return fail(LDPC_EINVAL, "NULL device pointer");
+    CU(cudaSetDevice(h->device));
+    WParams p;
+    wparams_fill(h, c, n, &p);
+    char* ws = static_cast<char*>(d_ws);
+    const size_t rb = c->fp64 ? 8 : 4;
+    p.llr = d_llr;
+    p.alpha = d_alpha;
+    p.beta = d_beta;
+    p.post = d_post;
+    p.ckpt = ws + lay.ckpt * rb;
+    p.rwork = ws + lay.rwork * rb;
+    if ((rc = weighted_forward(p, h->Z, h->D, (int)rb, static_cast<cudaStream_t>(stream), g_err))) return rc;
+    h->launches += n ? 1 : 0;
+    return 0;
+}
+
+extern "C" int ldpc_wdec_backward(ldpc_handle* h, const ldpc_wdec_config* c, int64_t n, const void* d_alpha,
+                                  const void* d_beta, const void* d_gpost, void* d_galpha, void* d_gbeta,
+                                  void* d_gllr, void* d_ws, void* stream) {
+    WLayout lay;
+    int rc;
+    if ((rc = wcheck(h, c, n, &lay))) return rc;
+    if (!d_alpha || !d_beta || !d_galpha || !d_gbeta || (n && (!d_gpost || !d_ws)))
+        return fail(LDPC_EINVAL, "NULL device pointer");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int rb = c->fp64 ? 8 : 4;
+    const size_t tc = (size_t)c->n_iter * c->n_classes * rb;
+    CU(cudaMemsetAsync(d_galpha, 0, tc, s));
+    CU(cudaMemsetAsync(d_gbeta, 0, tc, s));
+    WParams p;
+    wparams_fill(h, c, n, &p);
+    char* ws = static_cast<char*>(d_ws);
+    p.alpha = d_alpha;
+    p.beta = d_beta;
+    p.ckpt = ws + lay.ckpt * rb;
+    p.rwork = ws + lay.rwork * rb;
+    p.stash = ws + lay.stash * rb;
+    p.gr = ws + lay.gr * rb;
+    p.gpost = d_gpost;
+    p.galpha = d_galpha;
+    p.gbeta = d_gbeta;
+    p.gllr = d_gllr;
+    if ((rc = weighted_backward(p, h->Z, h->D, rb, s, g_err))) return rc;
+    h->launches += n ? 1 : 0;
     return 0;
 }

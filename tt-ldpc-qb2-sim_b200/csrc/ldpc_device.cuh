@@ -18,7 +18,7 @@
 namespace ldpcb200 {
 
 enum Storage : int { STORE_BF16 = 0, STORE_FP32 = 1, STORE_FP16 = 2 };
-enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1 };
+enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2 };
 
 // ------------------------------------------------------------------ Philox-4x32-10
 struct U32x4 { uint32_t x, y, z, w; };

@@ -59,6 +59,10 @@ struct QcParams {
     float ebn0_lo, ebn0_hi;               // per-frame Eb/N0 range in dB (used when hi > lo)
     float rate;                           // (N - M) / (N - P), for the per-frame mu and sigma
     unsigned long long* snr_bins;         // [4][SNR_BINS]: frames, frame errors, bit errors, iterations
+    // weighted Approximate-Min* (ALGO_WAMIN): check output sign * max(alpha * m - beta, 0)
+    const float2* wtab;                   // [w_iters][w_classes] (alpha, beta); iteration t uses row min(t, w_iters-1)
+    int32_t w_iters, w_classes;
+    int8_t w_class[QC_LAYERS][QC_DMAX];   // protograph edge class of edge e of layer l
 };
 
 enum TallyWord : int {
@@ -156,9 +160,12 @@ template <int d, int MODE> struct RowMsgGlobal {
 
 // Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
 // sL + f*lstride).  idx[e]: the row's column indices.
+// ALGO_WAMIN: wt[f] is slot f's row of (alpha, beta) pairs for its current iteration and cls[e] the
+// class of edge e.
 template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG>
 __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
-                                           MSG (&rm)[F], float r_cap, float lp_cap) {
+                                           MSG (&rm)[F], float r_cap, float lp_cap,
+                                           const float2* const* wt = nullptr, const int8_t* cls = nullptr) {
     using LT = LTraits<MODE>;
     float q[F][d];
 #pragma unroll
@@ -179,7 +186,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         // (9999 for Approximate-Min*, 999 for min-sum), the first minimum winning.
         bool is_am[d];
         float mag_min, mag_all;
-        if (ALGO == ALGO_AMIN) {
+        if (ALGO == ALGO_AMIN || ALGO == ALGO_WAMIN) {
             // Prefix minima pm_i = min(9999, |q_0|, .., |q_i|); mn = pm_{d-1}.  The argmin index am is
             // the first i with |q_i| = mn, so i < am exactly when pm_i > mn: no index is tracked.
             // The other edges in row order are o_i = |q_i| for i < am and |q_{i+1}| after it, and the
@@ -226,7 +233,12 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         float rn[d];
 #pragma unroll
         for (int e = 0; e < d; ++e) {
-            const uint32_t sel = is_am[e] ? smin : sall;
+            uint32_t sel = is_am[e] ? smin : sall;
+            if (ALGO == ALGO_WAMIN) {  // max(alpha * m - beta, 0): alpha = 1, beta = 0 leaves m unchanged
+                const float2 w = wt[f][cls[e]];
+                const float z = __fsub_rn(__fmul_rn(w.x, is_am[e] ? mag_min : mag_all), w.y);
+                sel = __float_as_uint(z > 0.0f ? z : 0.0f) | par;
+            }
             rn[e] = __uint_as_float(sel ^ (__float_as_uint(q[f][e]) & 0x80000000u));
             float ln = __fadd_rn(q[f][e], rn[e]);
             if (CLIP) ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
@@ -419,6 +431,9 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const int lstride = (N + 7) & ~7;                      // elements per slot (16-byte multiple)
     LE* sL = reinterpret_cast<LE*>(smem_raw);
     uint32_t* sHB = reinterpret_cast<uint32_t*>(smem_raw + (size_t)F * lstride * sizeof(LE));  // [F][nblk*W]
+    // ALGO_WAMIN: the weight table after the hard-decision words, 16-byte aligned
+    float2* sW = reinterpret_cast<float2*>(
+        smem_raw + (((size_t)F * lstride * sizeof(LE) + (size_t)F * (N / 32) * 4 + 15) & ~(size_t)15));
     __shared__ uint32_t s_fid[QC_MAX_F];
     __shared__ uint32_t s_sfail[QC_MAX_F];
     __shared__ uint32_t s_be[QC_MAX_F];
@@ -429,6 +444,9 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
 
     MsgRegs<D, R, F, MODE, PAIR, RG> msg;
+    if constexpr (ALGO == ALGO_WAMIN) {  // visible after the first refill's barrier
+        for (int i = tid; i < p.w_iters * p.w_classes; i += T) sW[i] = p.wtab[i];
+    }
 
     uint32_t act = 0;                // active slots (uniform)
     uint32_t need = (1u << F) - 1u;  // slots waiting for a frame (uniform)
@@ -514,6 +532,10 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
 
         // ---------------------------------------------------------------- one layered iteration
         if (p.max_iter > 0) {
+            const float2* wt[F];
+#pragma unroll
+            for (int f = 0; f < F; ++f)
+                wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_classes : nullptr;
 #pragma unroll
             for (int l = 0; l < QC_LAYERS; ++l) {
 #pragma unroll
@@ -530,11 +552,13 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                                 rm[f] = RowMsgGlobal<QC_DEG_LOW, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
                                         p.layer_off[l] + j, Z};
-                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap);
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wt,
+                                                                       p.w_class[l]);
                         } else if constexpr (PAIR)
                             row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
                         else
-                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap);
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap,
+                                                                       lp_cap, wt, p.w_class[l]);
                     } else {
                         int idx[D];
 #pragma unroll
@@ -546,11 +570,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                                 rm[f] = RowMsgGlobal<D, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
                                         p.layer_off[l] + j, Z};
-                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap);
+                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wt, p.w_class[l]);
                         } else if constexpr (PAIR)
                             row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
                         else
-                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap, lp_cap);
+                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap,
+                                                               lp_cap, wt, p.w_class[l]);
                     }
                 }
                 __syncthreads();

@@ -17,5 +17,9 @@ static const QcEntry qc_r12k4[] = {
     LDPC_QC_ENTRY(512, 6, 1, 1, STORE_BF16, ALGO_AMIN, true, true),
     LDPC_QC_ENTRY(512, 6, 1, 1, STORE_BF16, ALGO_NMS, false, true),
     LDPC_QC_ENTRY(512, 6, 1, 1, STORE_BF16, ALGO_NMS, true, true),
+    // weighted Approximate-Min* (trained weights, LDPC_ALGO_WAMIN): simulation and caller-supplied LLRs
+    LDPC_QC_ENTRY(512, 6, 1, 1, STORE_FP16, ALGO_WAMIN, false, false),
+    LDPC_QC_ENTRY(512, 6, 1, 1, STORE_FP16, ALGO_WAMIN, false, true),
+    LDPC_QC_ENTRY(512, 6, 1, 1, STORE_FP32, ALGO_WAMIN, false, true),
 };
 LDPC_QC_REGISTER(qc_r12k4)

@@ -233,6 +233,10 @@ class QcCode:
     N: int
     P: int
     layers: List[List[Tuple[int, int]]] = field(default_factory=list)
+    # protograph edge class of edge e of layer l: one class per edge of the base matrix (an "I" or a
+    # permutation P_k in block (row, column)), numbered row by row, column by column
+    edge_class: List[List[int]] = field(default_factory=list)
+    n_classes: int = 0
 
     @property
     def name(self) -> str:
@@ -305,13 +309,20 @@ def make_code(K: int, rate: str) -> QcCode:
     N = n_block_cols * M
     perms = {}
     layers: List[List[Tuple[int, int]]] = []
+    classes: List[List[int]] = []
+    class_id = {}
+    for b, brow in enumerate(layout):
+        for c, entry in enumerate(brow):
+            for pi, p in enumerate(_entry_perms(entry)):
+                class_id[(b, c, pi)] = len(class_id)
     for b, brow in enumerate(layout):
         for q in range(4):
             lay = []
             for c, entry in enumerate(brow):
-                for p in _entry_perms(entry):
+                for pi, p in enumerate(_entry_perms(entry)):
+                    cls = class_id[(b, c, pi)]
                     if p == "I":
-                        lay.append((4 * c + q, 0))
+                        lay.append((4 * c + q, 0, cls))
                     else:
                         if p not in perms:
                             perms[p] = permutation(p, M)
@@ -321,13 +332,15 @@ def make_code(K: int, rate: str) -> QcCode:
                         # the whole quarter must be one cyclic shift: pi(q*Z + j) = cq*Z + (j+s) % Z
                         j = np.arange(Z)
                         assert np.array_equal(pi[q * Z + j], cq * Z + (j + s) % Z)
-                        lay.append((4 * c + cq, s))
+                        lay.append((4 * c + cq, s, cls))
             lay.sort()
-            blocks = [bk for bk, _ in lay]
+            blocks = [bk for bk, _, _ in lay]
             if len(set(blocks)) != len(blocks):
                 raise AssertionError(f"layer {4 * b + q} of ({K},{rate}) has two circulants in one block")
-            layers.append(lay)
-    return QcCode(K=K, rate=rate, M=M, Z=Z, N=N, P=M, layers=layers)
+            layers.append([(bk, s) for bk, s, _ in lay])
+            classes.append([cl for _, _, cl in lay])
+    return QcCode(K=K, rate=rate, M=M, Z=Z, N=N, P=M, layers=layers, edge_class=classes,
+                  n_classes=len(class_id))
 
 
 def all_codes() -> List[QcCode]:

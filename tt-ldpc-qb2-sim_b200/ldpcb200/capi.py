@@ -16,13 +16,15 @@ import numpy as np
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libldpcb200.so")
 
 STORE_BF16, STORE_FP32, STORE_FP16 = 0, 1, 2
-ALGO_AMIN, ALGO_NMS = 0, 1
+ALGO_AMIN, ALGO_NMS, ALGO_WAMIN = 0, 1, 2
 KERNEL_QC, KERNEL_GENERAL = 0, 1
 STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
-           "ldpc_channel_llr", "ldpc_iter_histogram", "ldpc_snr_bins", "ldpc_set_launch_shape", "ldpc_list_shapes",
+           "ldpc_channel_llr", "ldpc_channel_llr_device", "ldpc_iter_histogram", "ldpc_snr_bins",
+           "ldpc_set_launch_shape", "ldpc_list_shapes", "ldpc_list_shapes_algo", "ldpc_set_weights",
+           "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
 
@@ -51,6 +53,12 @@ class RunParams(C.Structure):
 
 
 SNR_BINS = 32
+
+
+class WdecConfig(C.Structure):
+    _fields_ = [("n_iter", C.c_int32), ("n_classes", C.c_int32), ("ckpt_every", C.c_int32),
+                ("post_all", C.c_int32), ("fp64", C.c_int32), ("reserved0", C.c_int32),
+                ("edge_class", (C.c_int32 * 18) * 12)]
 
 
 class Tally(C.Structure):
@@ -91,6 +99,15 @@ def load(path: str = LIB_PATH):
     L.ldpc_batch_run.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), P(Tally), P(C.c_float)]
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
+    L.ldpc_list_shapes_algo.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int32), C.c_int]
+    L.ldpc_set_weights.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int, C.c_int, P(C.c_int32)]
+    L.ldpc_channel_llr_device.argtypes = [C.c_void_p, P(RunParams), C.c_void_p, C.c_void_p]
+    L.ldpc_wdec_workspace_bytes.argtypes = [C.c_void_p, P(WdecConfig), C.c_int64]
+    L.ldpc_wdec_workspace_bytes.restype = C.c_int64
+    L.ldpc_wdec_forward.argtypes = [C.c_void_p, P(WdecConfig), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ldpc_wdec_backward.argtypes = [C.c_void_p, P(WdecConfig), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.ldpc_launch_count.argtypes = [C.c_void_p]
     L.ldpc_launch_count.restype = C.c_int64
     L.ldpc_launch_param_bytes.argtypes = [C.c_void_p]
@@ -219,28 +236,29 @@ class Decoder:
         _check(self._lib.ldpc_set_launch_shape(self._h, storage, rows_per_thread, frames_per_cta, min_ctas_per_sm,
                                                global_messages))
 
-    def shapes(self, storage) -> list:
+    def shapes(self, storage, algo: int = ALGO_AMIN) -> list:
         """Built QC launch shapes (rows per thread, frames per CTA, min CTAs per SM, global messages)
-        for a storage mode."""
+        for a storage mode and algorithm."""
         if isinstance(storage, str):
             storage = STORAGE_NAMES[storage]
         buf = np.zeros(4 * 64, np.int32)
-        n = _check(self._lib.ldpc_list_shapes(self._h, storage, _ip(buf), 64))
+        n = _check(self._lib.ldpc_list_shapes_algo(self._h, storage, algo, _ip(buf), 64))
         return [tuple(int(x) for x in buf[4 * i:4 * i + 4]) for i in range(min(n, 64))]
 
     def autotune(self, mu: float, sigma: float, storages=("fp32", "fp16", "bf16"), frames: int = 1 << 18,
-                 max_iter: int = 200, seed: int = 0x5EED, repeats: int = 2):
+                 max_iter: int = 200, seed: int = 0x5EED, repeats: int = 2, algo: int = ALGO_AMIN):
         """Times every built launch shape of each storage mode on ``frames`` frames of this channel
         and keeps the fastest per mode.  Returns {storage: (best shape, {shape: Mframes/s})} and the
         fastest storage overall."""
         out = {}
         best_overall = None
         for st in storages:
-            shapes = self.shapes(st) if self.kind == KERNEL_QC else []
+            shapes = self.shapes(st, algo) if self.kind == KERNEL_QC else []
             timings = {}
             for sh in shapes:
                 self.set_launch_shape(*sh, storage=st)
-                p = self.params(mu=mu, sigma=sigma, seed=seed, n_frames=frames, max_iter=max_iter, storage=st)
+                p = self.params(mu=mu, sigma=sigma, seed=seed, n_frames=frames, max_iter=max_iter, storage=st,
+                                algo=algo)
                 self.run_chunk(p)  # warm-up
                 ms = min(self.run_chunk(p).kernel_ms for _ in range(repeats))
                 timings[sh] = frames / (ms * 1e-3) / 1e6
@@ -297,6 +315,24 @@ class Decoder:
         out = np.empty((int(p.n_frames), self.n_tx), np.float32)
         _check(self._lib.ldpc_channel_llr(self._h, C.byref(p), _fp(out)))
         return out
+
+    def channel_llr_device(self, p: RunParams, d_llr: int, stream: int = 0):
+        """ldpc_channel_llr into a device array (address as an integer) on a CUDA stream (handle as
+        an integer; 0 = the legacy default stream), without waiting."""
+        _check(self._lib.ldpc_channel_llr_device(self._h, C.byref(p), d_llr or None, stream or None))
+
+    def set_weights(self, alpha: np.ndarray, beta: np.ndarray, edge_class: np.ndarray):
+        """Weights of ALGO_WAMIN runs: alpha/beta [T][C] (iterations past T use row T-1),
+        edge_class [12][18]."""
+        a = np.ascontiguousarray(alpha, dtype=np.float32)
+        b = np.ascontiguousarray(beta, dtype=np.float32)
+        ec = np.ascontiguousarray(edge_class, dtype=np.int32)
+        if a.ndim != 2 or a.shape != b.shape or ec.shape != (12, 18):
+            raise ValueError("alpha/beta must be [T][C] and edge_class [12][18]")
+        _check(self._lib.ldpc_set_weights(self._h, _fp(a), _fp(b), a.shape[0], a.shape[1], _ip(ec)))
+
+    def clear_weights(self):
+        _check(self._lib.ldpc_set_weights(self._h, None, None, 0, 0, None))
 
     def iter_histogram(self, n_bins: int = 256) -> np.ndarray:
         h = np.zeros(n_bins, np.uint64)

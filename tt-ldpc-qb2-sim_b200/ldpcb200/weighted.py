@@ -1,0 +1,255 @@
+"""Weighted Approximate-Min* decoder: autograd function, trainable module and training loop.
+
+The decoder is the layered Approximate-Min* decoder of the simulation path with one change in the
+check-node output: r_e = sign_e * relu(alpha[t][c] * m_e - beta[t][c]), where m_e is the
+Approximate-Min* magnitude the plain decoder would send on edge e (ldpc_decoder_core.h:176-201 of
+the reference), t the iteration and c the protograph edge class of the edge (one class per edge of
+the AR4JA base matrix, ar4ja.QcCode.edge_class).  It runs exactly T iterations (no early stop), so
+it can be differentiated; the forward and the adjoint are hand-written CUDA kernels
+(csrc/weighted.cu) behind ``WeightedFn``, and the adjoint recomputes each segment of ``ckpt_every``
+iterations from an activation checkpoint.  With alpha = 1 and beta = 0 the forward pass gives the
+plain fp32 decoder's values bit for bit.
+
+Training (``train``) draws its frames from the simulator's own channel (Philox + Box-Muller AWGN,
+all-zero codeword, per-frame Eb/N0 uniform in a range), through ``ldpc_channel_llr_device``, and
+minimises the binary cross-entropy of the posteriors against the all-zero codeword,
+mean(softplus(-L)), averaged over all T iterations' posteriors.  Trained weights run in the
+simulation kernels as LDPC_ALGO_WAMIN (``Decoder.set_weights``), with the syndrome stop.  The
+reference has no weighted or trainable decoder; nothing here has a counterpart there.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import time
+from dataclasses import dataclass
+from typing import Callable, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import ar4ja, capi
+
+# channel stream id of the training frames (evaluation uses the simulation's streams 0..)
+TRAIN_STREAM = 0x7EA1
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+
+
+def edge_class_table(code: ar4ja.QcCode) -> np.ndarray:
+    """[12][18] int32: class of edge e of layer l (0 beyond the layer's degree)."""
+    t = np.zeros((12, 18), np.int32)
+    for l, cls in enumerate(code.edge_class):
+        t[l, :len(cls)] = cls
+    return t
+
+
+def make_config(code: ar4ja.QcCode, n_iter: int, ckpt_every: int = 5, post_all: bool = True,
+                fp64: bool = False) -> capi.WdecConfig:
+    c = capi.WdecConfig()
+    c.n_iter, c.n_classes, c.ckpt_every = int(n_iter), int(code.n_classes), int(min(ckpt_every, n_iter))
+    c.post_all, c.fp64 = int(bool(post_all)), int(bool(fp64))
+    tab = edge_class_table(code)
+    for l in range(12):
+        for e in range(18):
+            c.edge_class[l][e] = int(tab[l, e])
+    return c
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return t.data_ptr() if t is not None else None
+
+
+class WeightedFn(torch.autograd.Function):
+    """posteriors = WeightedFn.apply(llr, alpha, beta, decoder, config).
+
+    llr [B][N-P], alpha/beta [T][C] on the decoder's GPU, float32 (or float64 with config.fp64);
+    returns [T][B][N] (post_all) or [1][B][N].  Gradients flow to llr, alpha and beta."""
+
+    @staticmethod
+    def forward(ctx, llr, alpha, beta, dec: capi.Decoder, cfg: capi.WdecConfig):
+        dt = torch.float64 if cfg.fp64 else torch.float32
+        for name, t in (("llr", llr), ("alpha", alpha), ("beta", beta)):
+            if not t.is_cuda or t.dtype != dt:
+                raise ValueError(f"{name} must be a CUDA {dt} tensor")
+        llr, alpha, beta = llr.contiguous(), alpha.contiguous(), beta.contiguous()
+        B = int(llr.shape[0])
+        if llr.shape[1] != dec.n_tx or tuple(alpha.shape) != (cfg.n_iter, cfg.n_classes) or alpha.shape != beta.shape:
+            raise ValueError("shape mismatch")
+        lib = dec._lib
+        nbytes = capi._check(int(lib.ldpc_wdec_workspace_bytes(dec._h, C.byref(cfg), B)))
+        ws = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=llr.device)
+        post = torch.empty((cfg.n_iter if cfg.post_all else 1, B, dec.N), dtype=dt, device=llr.device)
+        stream = torch.cuda.current_stream(llr.device).cuda_stream
+        capi._check(lib.ldpc_wdec_forward(dec._h, C.byref(cfg), _ptr(llr), B, _ptr(alpha), _ptr(beta), _ptr(post),
+                                          _ptr(ws), stream or None))
+        ctx.dec, ctx.cfg, ctx.ws, ctx.B = dec, cfg, ws, B
+        ctx.save_for_backward(alpha, beta)
+        ctx.llr_shape = tuple(llr.shape)
+        return post
+
+    @staticmethod
+    def backward(ctx, gpost):
+        alpha, beta = ctx.saved_tensors
+        dec, cfg = ctx.dec, ctx.cfg
+        gpost = gpost.contiguous()
+        galpha, gbeta = torch.empty_like(alpha), torch.empty_like(beta)
+        gllr = torch.empty(ctx.llr_shape, dtype=alpha.dtype, device=alpha.device) if ctx.needs_input_grad[0] else None
+        stream = torch.cuda.current_stream(alpha.device).cuda_stream
+        capi._check(dec._lib.ldpc_wdec_backward(dec._h, C.byref(cfg), ctx.B, _ptr(alpha), _ptr(beta), _ptr(gpost),
+                                                _ptr(galpha), _ptr(gbeta), _ptr(gllr), _ptr(ctx.ws), stream or None))
+        ctx.ws = None
+        return gllr, galpha, gbeta, None, None
+
+
+def extend(w: torch.Tensor, n_iter: int) -> torch.Tensor:
+    """Parameters of T' iterations from trained ones of T: cut, or repeat the last iteration's."""
+    if w.shape[0] >= n_iter:
+        return w[:n_iter]
+    return torch.cat([w, w[-1:].expand(n_iter - w.shape[0], -1)], 0)
+
+
+class WeightedDecoder(torch.nn.Module):
+    """Trainable weighted decoder of one AR4JA code (makeH row order): parameters alpha and beta of
+    shape [T][C], initialised to 1 and 0 (the plain decoder)."""
+
+    def __init__(self, code: ar4ja.QcCode, n_iter: int = 20, ckpt_every: int = 5, device: int = 0,
+                 dtype: torch.dtype = torch.float32, post_all: bool = True):
+        super().__init__()
+        self.code, self.n_iter, self.device = code, int(n_iter), torch.device("cuda", device)
+        self.dec = capi.Decoder.from_code(code, device)
+        self.cfg = make_config(code, n_iter, ckpt_every, post_all, dtype == torch.float64)
+        self.alpha = torch.nn.Parameter(torch.ones(n_iter, code.n_classes, dtype=dtype, device=self.device))
+        self.beta = torch.nn.Parameter(torch.zeros(n_iter, code.n_classes, dtype=dtype, device=self.device))
+
+    def forward(self, llr: torch.Tensor) -> torch.Tensor:
+        return WeightedFn.apply(llr, self.alpha, self.beta, self.dec, self.cfg)
+
+    def channel(self, n_frames: int, ebn0: Tuple[float, float], seed: int, first_frame: int = 0,
+                stream_id: int = TRAIN_STREAM, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Channel LLRs [n][N-P] (float32, on the GPU) from the simulator's channel kernel: all-zero
+        codeword, BPSK, AWGN with per-frame Eb/N0 uniform in [ebn0[0], ebn0[1]) dB."""
+        if out is None:
+            out = torch.empty((n_frames, self.dec.n_tx), dtype=torch.float32, device=self.device)
+        lo, hi = float(ebn0[0]), float(ebn0[1])
+        if hi > lo:
+            p = self.dec.params(seed=seed, stream=stream_id, first_frame=first_frame, n_frames=n_frames,
+                                ebn0_lo=lo, ebn0_hi=hi)
+        else:
+            mu, sigma = capi.channel_mu_sigma(self.code.N, self.code.n_checks, self.code.P, lo)
+            p = self.dec.params(mu=mu, sigma=sigma, seed=seed, stream=stream_id, first_frame=first_frame,
+                                n_frames=n_frames)
+        self.dec.channel_llr_device(p, out.data_ptr(), torch.cuda.current_stream(self.device).cuda_stream)
+        return out
+
+    def state(self) -> dict:
+        return {"code": self.code.name, "K": self.code.K, "rate": self.code.rate, "n_iter": self.n_iter,
+                "n_classes": self.code.n_classes,
+                "alpha": self.alpha.detach().double().cpu().numpy().round(7).tolist(),
+                "beta": self.beta.detach().double().cpu().numpy().round(7).tolist()}
+
+    def load_state(self, st: dict):
+        a = torch.tensor(st["alpha"], dtype=self.alpha.dtype)
+        b = torch.tensor(st["beta"], dtype=self.beta.dtype)
+        with torch.no_grad():
+            self.alpha.copy_(extend(a, self.n_iter))
+            self.beta.copy_(extend(b, self.n_iter))
+
+    def close(self):
+        self.dec.close()
+
+
+def bce_allzero(post: torch.Tensor) -> torch.Tensor:
+    """Binary cross-entropy of posterior LLRs (positive = bit 0) against the all-zero codeword."""
+    return torch.nn.functional.softplus(-post).mean()
+
+
+@dataclass
+class TrainLog:
+    step: int
+    loss: float
+    seconds: float
+
+
+def train(code: ar4ja.QcCode, steps: int = 5000, batch: int = 4096, ebn0: Tuple[float, float] = (1.0, 2.5),
+          lr: float = 1e-3, n_iter: int = 20, ckpt_every: int = 5, seed: int = 1, device: int = 0,
+          log_every: int = 100, callback: Optional[Callable[[TrainLog], None]] = None) -> Tuple[WeightedDecoder, list]:
+    """Adam on mean BCE over all iterations' posteriors; step i decodes frames i * batch .. of the
+    training channel stream, so every step sees fresh frames."""
+    torch.cuda.set_device(device)
+    model = WeightedDecoder(code, n_iter, ckpt_every, device)
+    opt = torch.optim.Adam(model.parameters(), lr=lr)
+    llr = torch.empty((batch, model.dec.n_tx), dtype=torch.float32, device=model.device)
+    log = []
+    t0 = time.time()
+    for step in range(steps):
+        model.channel(batch, ebn0, seed, first_frame=step * batch, out=llr)
+        loss = bce_allzero(model(llr))
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        opt.step()
+        if log_every and (step % log_every == 0 or step == steps - 1):
+            entry = TrainLog(step, float(loss.item()), time.time() - t0)
+            log.append(entry)
+            if callback:
+                callback(entry)
+    torch.cuda.synchronize(device)
+    return model, log
+
+
+def weights_path(code: ar4ja.QcCode, n_iter: int) -> str:
+    return os.path.join(WEIGHTS_DIR, f"ar4ja_r{code.rate.replace('/', '')}_k{code.K}_t{n_iter}.json")
+
+
+def save_weights(model: WeightedDecoder, path: str, extra: Optional[dict] = None):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    st = model.state()
+    st.update(extra or {})
+    with open(path, "w") as f:
+        json.dump(st, f, indent=1)
+
+
+def load_weights(path: str) -> dict:
+    with open(path) as f:
+        return json.load(f)
+
+
+def apply_weights(dec: capi.Decoder, code: ar4ja.QcCode, st: dict, n_iter: Optional[int] = None):
+    """Loads trained weights into a simulation decoder (ALGO_WAMIN runs); n_iter extends or cuts the
+    table (iterations past the trained ones reuse the last trained iteration's weights)."""
+    a = np.asarray(st["alpha"], np.float32)
+    b = np.asarray(st["beta"], np.float32)
+    if n_iter:
+        a = extend(torch.from_numpy(a), n_iter).numpy()
+        b = extend(torch.from_numpy(b), n_iter).numpy()
+    dec.set_weights(a, b, edge_class_table(code))
+
+
+def _main(argv: Optional[Sequence[str]] = None):
+    import argparse
+    ap = argparse.ArgumentParser(description="Train the weighted Approximate-Min* decoder of an AR4JA code")
+    ap.add_argument("--K", type=int, default=1024)
+    ap.add_argument("--rate", default="1/2")
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--ckpt-every", type=int, default=5)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--ebn0", type=float, nargs=2, default=(1.0, 2.5))
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default="")
+    a = ap.parse_args(argv)
+    code = ar4ja.make_code(a.K, a.rate)
+    model, log = train(code, a.steps, a.batch, tuple(a.ebn0), a.lr, a.iters, a.ckpt_every, a.seed, a.device,
+                       callback=lambda e: print(json.dumps(e.__dict__), flush=True))
+    out = a.out or weights_path(code, a.iters)
+    save_weights(model, out, {"train": {"steps": a.steps, "batch": a.batch, "ebn0_db": list(a.ebn0), "lr": a.lr,
+                                        "ckpt_every": a.ckpt_every, "seed": a.seed,
+                                        "loss": [[e.step, round(e.loss, 6)] for e in log],
+                                        "seconds": round(log[-1].seconds, 2) if log else 0.0}})
+    print(json.dumps({"saved": out}))
+
+
+if __name__ == "__main__":
+    _main()
