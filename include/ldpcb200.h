@@ -194,8 +194,9 @@ int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const
  * arrays, copied): alpha/beta [n_iter][n_classes] (iteration t >= n_iter uses row n_iter - 1) and
  * edge_class [12][18], the class of edge e of layer l.  The check-node output becomes
  * sign * max(alpha[t][c] * m - beta[t][c], 0) in the simulation kernels (with syndrome stop and
- * tallies, like every other algorithm).  n_iter = 0 removes the weights.  QC codes only; no clips.
- * No counterpart in the reference. */
+ * tallies, like every other algorithm).  The table is expanded to one pair per iteration and edge of a
+ * row-layer set, n_iter x (12 + 8 D) x 8 bytes, at most 64 KB (n_iter <= 52 for D = 18).
+ * n_iter = 0 removes the weights.  QC codes only; no clips.  No counterpart in the reference. */
 int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float* beta, int n_iter, int n_classes,
                      const int32_t* edge_class);
 

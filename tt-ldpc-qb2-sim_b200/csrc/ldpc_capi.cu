@@ -91,9 +91,8 @@ struct ldpc_handle {
     int32_t* d_frame_out = nullptr;  // 3 * cap
     size_t frame_cap = 0;
     // weights of LDPC_ALGO_WAMIN runs
-    float2* d_wtab = nullptr;  // [w_iters][w_classes] (alpha, beta)
-    int w_iters = 0, w_classes = 0;
-    int8_t w_class[QC_LAYERS][QC_DMAX] = {};
+    float2* d_wtab = nullptr;  // [w_iters][w_slots] (alpha, beta) per iteration and edge slot
+    int w_iters = 0, w_slots = 0;
     unsigned long long* h_tally = nullptr;  // pinned
     int64_t launches = 0;
 };
@@ -286,31 +285,33 @@ extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float*
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
     if (!alpha || !beta || !edge_class || n_iter < 0 || n_iter > 1000 || n_classes < 1 || n_classes > 127)
         return fail(LDPC_EINVAL, "bad weights (n_iter %d, n_classes %d)", n_iter, n_classes);
-    int8_t cls[QC_LAYERS][QC_DMAX] = {};
+    // expand the class table to one (alpha, beta) pair per edge slot and iteration, so the kernel
+    // addresses a layer's weights at constant offsets
+    const int slots = QC_DEG_LOW * 4 + h->D * 8;
     for (int l = 0; l < QC_LAYERS; ++l)
-        for (int e = 0; e < QC_DMAX; ++e) {
+        for (int e = 0; e < (l < 4 ? QC_DEG_LOW : h->D); ++e) {
             const int32_t c = edge_class[l * QC_DMAX + e];
-            const bool used = e < (l < 4 ? QC_DEG_LOW : h->D);
-            if (used && (c < 0 || c >= n_classes))
-                return fail(LDPC_EINVAL, "edge class of layer %d edge %d out of range", l, e);
-            cls[l][e] = used ? (int8_t)c : 0;
+            if (c < 0 || c >= n_classes) return fail(LDPC_EINVAL, "edge class of layer %d edge %d out of range", l, e);
         }
-    const size_t cnt = (size_t)n_iter * n_classes;
-    if (cnt * sizeof(float2) > 64 * 1024) return fail(LDPC_EINVAL, "weight table above 64 KB");
+    const size_t cnt = (size_t)n_iter * slots;
+    if (cnt * sizeof(float2) > 64 * 1024)
+        return fail(LDPC_EINVAL, "weight table of %d iterations x %d edge slots is above 64 KB", n_iter, slots);
     std::vector<float2> tab(cnt);
-    for (size_t i = 0; i < cnt; ++i) {
-        if (!(alpha[i] == alpha[i]) || !(beta[i] == beta[i])) return fail(LDPC_EINVAL, "NaN weight");
-        tab[i] = make_float2(alpha[i], beta[i]);
-    }
+    for (int t = 0; t < n_iter; ++t)
+        for (int l = 0; l < QC_LAYERS; ++l)
+            for (int e = 0; e < (l < 4 ? QC_DEG_LOW : h->D); ++e) {
+                const size_t k = (size_t)t * n_classes + edge_class[l * QC_DMAX + e];
+                if (!(alpha[k] == alpha[k]) || !(beta[k] == beta[k])) return fail(LDPC_EINVAL, "NaN weight");
+                tab[(size_t)t * slots + qc_edge_slot(l, e, h->D)] = make_float2(alpha[k], beta[k]);
+            }
     CU(cudaSetDevice(h->device));
     cudaFree(h->d_wtab);
     h->d_wtab = nullptr;
     h->w_iters = 0;
     CU(cudaMalloc(&h->d_wtab, cnt * sizeof(float2)));
     CU(cudaMemcpy(h->d_wtab, tab.data(), cnt * sizeof(float2), cudaMemcpyHostToDevice));
-    memcpy(h->w_class, cls, sizeof cls);
     h->w_iters = n_iter;
-    h->w_classes = n_classes;
+    h->w_slots = slots;
     return 0;
 }
 
@@ -444,8 +445,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     if (p->algo == LDPC_ALGO_WAMIN) {
         qp.wtab = h->d_wtab;
         qp.w_iters = h->w_iters;
-        qp.w_classes = h->w_classes;
-        memcpy(qp.w_class, h->w_class, sizeof qp.w_class);
+        qp.w_slots = h->w_slots;
     }
     const int T = h->Z / R;
     int32_t off = 0;
@@ -457,7 +457,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;
     const size_t lstride = (size_t)((h->N + 7) & ~7);
     size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
-    if (p->algo == LDPC_ALGO_WAMIN) smem = ((smem + 15) & ~(size_t)15) + (size_t)h->w_iters * h->w_classes * sizeof(float2);
+    if (p->algo == LDPC_ALGO_WAMIN) smem = ((smem + 15) & ~(size_t)15) + (size_t)h->w_iters * h->w_slots * sizeof(float2);
     if (smem > 48 * 1024) CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));

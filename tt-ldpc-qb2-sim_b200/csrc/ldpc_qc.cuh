@@ -60,10 +60,16 @@ struct QcParams {
     float rate;                           // (N - M) / (N - P), for the per-frame mu and sigma
     unsigned long long* snr_bins;         // [4][SNR_BINS]: frames, frame errors, bit errors, iterations
     // weighted Approximate-Min* (ALGO_WAMIN): check output sign * max(alpha * m - beta, 0)
-    const float2* wtab;                   // [w_iters][w_classes] (alpha, beta); iteration t uses row min(t, w_iters-1)
-    int32_t w_iters, w_classes;
-    int8_t w_class[QC_LAYERS][QC_DMAX];   // protograph edge class of edge e of layer l
+    // (alpha, beta) per iteration and edge slot: [w_iters][w_slots], edge e of layer l at slot
+    // qc_edge_slot(l, e, D); iteration t uses row min(t, w_iters - 1)
+    const float2* wtab;
+    int32_t w_iters, w_slots;
 };
+
+// Slot of edge e of layer l in a per-iteration row of the weight table: layers 0-3 (degree 3) first.
+__host__ __device__ constexpr int qc_edge_slot(int l, int e, int D) {
+    return l < 4 ? QC_DEG_LOW * l + e : QC_DEG_LOW * 4 + D * (l - 4) + e;
+}
 
 enum TallyWord : int {
     T_FRAMES = 0, T_BIT_ERR, T_FRAME_ERR, T_ITER_SUM, T_UNCONVERGED, T_MAX_ITER, T_BIT_ERR_SQ, TALLY_WORDS = 8
@@ -160,12 +166,12 @@ template <int d, int MODE> struct RowMsgGlobal {
 
 // Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
 // sL + f*lstride).  idx[e]: the row's column indices.
-// ALGO_WAMIN: wt[f] is slot f's row of (alpha, beta) pairs for its current iteration and cls[e] the
-// class of edge e.
+// ALGO_WAMIN: wt[f] points at the (alpha, beta) pairs of this layer's edges for slot f's current
+// iteration (edge e at wt[f][e]: a constant offset, no class lookup).
 template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG>
 __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
                                            MSG (&rm)[F], float r_cap, float lp_cap,
-                                           const float2* const* wt = nullptr, const int8_t* cls = nullptr) {
+                                           const float2* const* wt = nullptr) {
     using LT = LTraits<MODE>;
     float q[F][d];
 #pragma unroll
@@ -235,7 +241,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         for (int e = 0; e < d; ++e) {
             uint32_t sel = is_am[e] ? smin : sall;
             if (ALGO == ALGO_WAMIN) {  // max(alpha * m - beta, 0): alpha = 1, beta = 0 leaves m unchanged
-                const float2 w = wt[f][cls[e]];
+                const float2 w = wt[f][e];
                 const float z = __fsub_rn(__fmul_rn(w.x, is_am[e] ? mag_min : mag_all), w.y);
                 sel = __float_as_uint(z > 0.0f ? z : 0.0f) | par;
             }
@@ -445,7 +451,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
 
     MsgRegs<D, R, F, MODE, PAIR, RG> msg;
     if constexpr (ALGO == ALGO_WAMIN) {  // visible after the first refill's barrier
-        for (int i = tid; i < p.w_iters * p.w_classes; i += T) sW[i] = p.wtab[i];
+        for (int i = tid; i < p.w_iters * p.w_slots; i += T) sW[i] = p.wtab[i];
     }
 
     uint32_t act = 0;                // active slots (uniform)
@@ -535,9 +541,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             const float2* wt[F];
 #pragma unroll
             for (int f = 0; f < F; ++f)
-                wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_classes : nullptr;
+                wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_slots : nullptr;
 #pragma unroll
             for (int l = 0; l < QC_LAYERS; ++l) {
+                const float2* wl[F];
+#pragma unroll
+                for (int f = 0; f < F; ++f) wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(l, 0, D) : nullptr;
 #pragma unroll
                 for (int rho = 0; rho < R; ++rho) {
                     const int j = tid + rho * T;
@@ -552,13 +561,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                                 rm[f] = RowMsgGlobal<QC_DEG_LOW, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
                                         p.layer_off[l] + j, Z};
-                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wt,
-                                                                       p.w_class[l]);
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
                             row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
                         else
                             row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap,
-                                                                       lp_cap, wt, p.w_class[l]);
+                                                                       lp_cap, wl);
                     } else {
                         int idx[D];
 #pragma unroll
@@ -570,12 +578,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                                 rm[f] = RowMsgGlobal<D, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
                                         p.layer_off[l] + j, Z};
-                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wt, p.w_class[l]);
+                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
                             row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
                         else
                             row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap,
-                                                               lp_cap, wt, p.w_class[l]);
+                                                               lp_cap, wl);
                     }
                 }
                 __syncthreads();

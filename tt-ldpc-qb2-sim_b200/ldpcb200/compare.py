@@ -33,7 +33,9 @@ SEED = 0xC0DE5
 PLAIN_ITERS = 200
 
 
-def _weights_for(code: ar4ja.QcCode, cap: int) -> Tuple[dict, str]:
+def _weights_for(code: ar4ja.QcCode, cap: int, override: Optional[str] = None) -> Tuple[dict, str]:
+    if override:
+        return weighted.load_weights(override), os.path.basename(override)
     exact = weighted.weights_path(code, cap)
     if os.path.exists(exact):
         return weighted.load_weights(exact), os.path.basename(exact)
@@ -50,7 +52,8 @@ def _tune(dec: capi.Decoder, code: ar4ja.QcCode, ebn0: float, max_iter: int, alg
 
 
 def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps: Sequence[int],
-                 time_frames: int, device: int = 0, log=print, min_errors: int = 1000) -> dict:
+                 time_frames: int, device: int = 0, log=print, min_errors: int = 1000,
+                 weights: Optional[str] = None) -> dict:
     decs: List[capi.Decoder] = []
     names: List[str] = []
     iters: List[int] = []
@@ -66,7 +69,7 @@ def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps:
         algos.append(capi.ALGO_AMIN); storages.append(st)
         for cap in caps:
             d = capi.Decoder.from_code(code, device)
-            w, src = _weights_for(code, cap)
+            w, src = _weights_for(code, cap, weights)
             weighted.apply_weights(d, code, w, cap)
             st, _ = _tune(d, code, mid, cap, capi.ALGO_WAMIN, tune_frames)
             decs.append(d); names.append(f"weighted_t{cap}"); iters.append(cap)
@@ -142,6 +145,7 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
     ap.add_argument("--min-errors", type=int, default=1000,
                     help="stop a point once every decoder has this many frame errors")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--weights", default="", help="weights file to use instead of the committed ones")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     results = []
@@ -149,7 +153,8 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
         K, rate = spec.split(":")
         code = ar4ja.make_code(int(K), rate)
         results.append(compare_code(code, a.ebn0, a.frames, a.caps, a.time_frames, a.device,
-                                    log=lambda s: print(s, flush=True), min_errors=a.min_errors))
+                                    log=lambda s: print(s, flush=True), min_errors=a.min_errors,
+                                    weights=a.weights or None))
     doc = {"seed": SEED, "plain_max_iter": PLAIN_ITERS, "caps": a.caps, "max_frames_per_point": a.frames,
            "min_errors": a.min_errors, "results": results}
     if a.out:

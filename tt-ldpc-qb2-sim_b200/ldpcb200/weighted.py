@@ -159,8 +159,11 @@ class WeightedDecoder(torch.nn.Module):
         self.dec.close()
 
 
-def bce_allzero(post: torch.Tensor) -> torch.Tensor:
-    """Binary cross-entropy of posterior LLRs (positive = bit 0) against the all-zero codeword."""
+def bce_allzero(post: torch.Tensor, iters: Optional[Tuple[int, int]] = None) -> torch.Tensor:
+    """Binary cross-entropy of posterior LLRs (positive = bit 0) against the all-zero codeword, over
+    all iterations' posteriors [T][B][N] or only those of iterations iters[0]..iters[1] (1-based)."""
+    if iters is not None:
+        post = post[iters[0] - 1:iters[1]]
     return torch.nn.functional.softplus(-post).mean()
 
 
@@ -173,9 +176,11 @@ class TrainLog:
 
 def train(code: ar4ja.QcCode, steps: int = 5000, batch: int = 4096, ebn0: Tuple[float, float] = (1.0, 2.5),
           lr: float = 1e-3, n_iter: int = 20, ckpt_every: int = 5, seed: int = 1, device: int = 0,
-          log_every: int = 100, callback: Optional[Callable[[TrainLog], None]] = None) -> Tuple[WeightedDecoder, list]:
-    """Adam on mean BCE over all iterations' posteriors; step i decodes frames i * batch .. of the
-    training channel stream, so every step sees fresh frames."""
+          log_every: int = 100, callback: Optional[Callable[[TrainLog], None]] = None,
+          loss_iters: Optional[Tuple[int, int]] = None) -> Tuple[WeightedDecoder, list]:
+    """Adam on mean BCE over all iterations' posteriors (or those of loss_iters, 1-based inclusive);
+    step i decodes frames i * batch .. of the training channel stream, so every step sees fresh
+    frames."""
     torch.cuda.set_device(device)
     model = WeightedDecoder(code, n_iter, ckpt_every, device)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
@@ -184,7 +189,7 @@ def train(code: ar4ja.QcCode, steps: int = 5000, batch: int = 4096, ebn0: Tuple[
     t0 = time.time()
     for step in range(steps):
         model.channel(batch, ebn0, seed, first_frame=step * batch, out=llr)
-        loss = bce_allzero(model(llr))
+        loss = bce_allzero(model(llr), loss_iters)
         opt.zero_grad(set_to_none=True)
         loss.backward()
         opt.step()
@@ -238,14 +243,18 @@ def _main(argv: Optional[Sequence[str]] = None):
     ap.add_argument("--ebn0", type=float, nargs=2, default=(1.0, 2.5))
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--loss-iters", type=int, nargs=2, default=None,
+                    help="train on the posteriors of these iterations only (1-based, inclusive)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     code = ar4ja.make_code(a.K, a.rate)
+    li = tuple(a.loss_iters) if a.loss_iters else None
     model, log = train(code, a.steps, a.batch, tuple(a.ebn0), a.lr, a.iters, a.ckpt_every, a.seed, a.device,
-                       callback=lambda e: print(json.dumps(e.__dict__), flush=True))
+                       callback=lambda e: print(json.dumps(e.__dict__), flush=True), loss_iters=li)
     out = a.out or weights_path(code, a.iters)
     save_weights(model, out, {"train": {"steps": a.steps, "batch": a.batch, "ebn0_db": list(a.ebn0), "lr": a.lr,
                                         "ckpt_every": a.ckpt_every, "seed": a.seed,
+                                        "loss_iters": list(li) if li else "all",
                                         "loss": [[e.step, round(e.loss, 6)] for e in log],
                                         "seconds": round(log[-1].seconds, 2) if log else 0.0}})
     print(json.dumps({"saved": out}))
