@@ -145,8 +145,9 @@ int ldpc_snr_bins(ldpc_handle* h, uint64_t* out);
 
 /* Launch shape of the QC kernel's simulation path for one storage mode (-1 = all): rows per thread,
  * frames per CTA, the resident CTAs per SM its register allocation must allow (a register cap;
- * 0 = the compiler's choice), and whether the check messages live in global memory instead of
- * registers (1 for codes too large for the register file).  All zero restores the default.
+ * 0 = the compiler's choice), and the layout (global_messages): 0 = check messages in registers,
+ * 1 = in global memory (codes too large for the register file), 2 = in registers, with each
+ * thread's column offsets precomputed in shared memory.  All zero restores the default.
  * LDPC_ENOTSUP if the shape is not built for this code.  Used by the autotuner
  * (ldpcb200.capi.Decoder.autotune).  Options with no QC variant built (e.g. clips on a K = 16384
  * code) run on the general kernel. */
@@ -154,7 +155,7 @@ int ldpc_set_launch_shape(ldpc_handle* h, int storage, int rows_per_thread, int 
                           int min_ctas_per_sm, int global_messages);
 
 /* The QC shapes built for this code and storage mode: writes up to max_shapes quadruples
- * (rows per thread, frames per CTA, min CTAs per SM, global messages) and returns how many exist. */
+ * (rows per thread, frames per CTA, min CTAs per SM, layout) and returns how many exist. */
 int ldpc_list_shapes(const ldpc_handle* h, int storage, int32_t* shapes, int max_shapes);
 
 /* As ldpc_list_shapes for the simulation variants of one algorithm (LDPC_ALGO_*). */

@@ -225,3 +225,32 @@ def test_options_without_qc_variant_use_general_kernel(gpu):
     assert np.array_equal(it, oit) and np.array_equal(be, obe)
     assert np.array_equal(_bits(post), _bits(opost))
     _check_tally(tal, it, sf, be)
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+def test_offset_table_layout_matches_oracle(dec_r12k1, storage):
+    """Layout 2 (each thread's column offsets precomputed in shared memory): the same bits as the
+    oracle, and the same simulation tallies as the default layout in every built shape."""
+    c = ar4ja.make_code(1024, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.25)
+    rng = np.random.default_rng(len(storage) + 77)
+    llr = (mu + sigma * rng.standard_normal((20, c.n_tx))).astype(np.float32)
+    p = dec_r12k1.params(mu=mu, sigma=sigma, seed=6, first_frame=3, n_frames=4001, max_iter=200, storage=storage)
+    plain = dec_r12k1.run_chunk(p)
+    shapes = [s_ for s_ in dec_r12k1.shapes(storage) if s_[3] == 2]
+    assert shapes
+    try:
+        dec_r12k1.set_launch_shape(1, 1, 0, 2, storage=storage)
+        post, it, sf, be, tal = dec_r12k1.decode_llr(llr, max_iter=60, storage=storage)
+        for sh in shapes:
+            dec_r12k1.set_launch_shape(*sh, storage=storage)
+            ot = dec_r12k1.run_chunk(p)
+            for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters", "bit_errors_sq"):
+                assert getattr(ot, k) == getattr(plain, k), (sh, k)
+    finally:
+        dec_r12k1.set_launch_shape(0, 0, 0, 0, storage=storage)
+    mode = {"bf16": O.STORE_BF16, "fp32": O.STORE_FP32, "fp16": O.STORE_FP16}[storage]
+    opost, oit, osf, obe = O.decode(O.Code(c.row_matrix(), c.N, c.P), llr, mode=mode, max_iter=60)
+    assert np.array_equal(it, oit) and np.array_equal(be, obe) and np.array_equal(sf, osf)
+    assert np.array_equal(_bits(post), _bits(opost))
+    _check_tally(tal, it, sf, be)

@@ -318,7 +318,7 @@ extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float*
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 1)
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 2)
         return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
@@ -456,8 +456,11 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     qp.slot_elems = off;
     const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;
     const size_t lstride = (size_t)((h->N + 7) & ~7);
+    // the kernel's layout: L slots, hard-decision words, [16-byte aligned] offset table (G = 2), weights
     size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
-    if (p->algo == LDPC_ALGO_WAMIN) smem = ((smem + 15) & ~(size_t)15) + (size_t)h->w_iters * h->w_slots * sizeof(float2);
+    if (G == 2 || p->algo == LDPC_ALGO_WAMIN) smem = (smem + 15) & ~(size_t)15;
+    if (G == 2) smem += (size_t)T * (QC_DEG_LOW * 4 + h->D * 8) * 4;
+    if (p->algo == LDPC_ALGO_WAMIN) smem += (size_t)h->w_iters * h->w_slots * sizeof(float2);
     if (smem > 48 * 1024) CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
@@ -470,7 +473,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     out->block = T;
     out->smem = smem;
     if (grid == 0) return 0;
-    if (G) {
+    if (G == 1) {
         int rc;
         const size_t rsz = p->storage == LDPC_STORE_FP32 ? 4 : 2;
         if ((rc = ensure_cap(&h->d_rmsg, &h->rmsg_cap, grid * F * (size_t)qp.slot_elems * rsz))) return rc;

@@ -168,16 +168,23 @@ template <int d, int MODE> struct RowMsgGlobal {
 // sL + f*lstride).  idx[e]: the row's column indices.
 // ALGO_WAMIN: wt[f] points at the (alpha, beta) pairs of this layer's edges for slot f's current
 // iteration (edge e at wt[f][e]: a constant offset, no class lookup).
-template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG>
+// BO: idx[e] holds byte offsets into the slot's L array instead of element indices (the column
+// offset table of the OT layout), so no index scaling is needed.
+template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG, bool BO = false>
 __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
                                            MSG (&rm)[F], float r_cap, float lp_cap,
                                            const float2* const* wt = nullptr) {
     using LT = LTraits<MODE>;
+    using LE = typename LT::T;
+    auto lptr = [&](int f, int e) -> LE* {
+        if constexpr (BO) return reinterpret_cast<LE*>(reinterpret_cast<char*>(sL + f * lstride) + idx[e]);
+        else return sL + f * lstride + idx[e];
+    };
     float q[F][d];
 #pragma unroll
     for (int f = 0; f < F; ++f)
 #pragma unroll
-        for (int e = 0; e < d; ++e) q[f][e] = __fsub_rn(LT::ld(sL + f * lstride, idx[e]), rm[f].get(e));
+        for (int e = 0; e < d; ++e) q[f][e] = __fsub_rn(LT::ld(lptr(f, e), 0), rm[f].get(e));
 
 #pragma unroll
     for (int f = 0; f < F; ++f) {
@@ -248,7 +255,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
             rn[e] = __uint_as_float(sel ^ (__float_as_uint(q[f][e]) & 0x80000000u));
             float ln = __fadd_rn(q[f][e], rn[e]);
             if (CLIP) ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
-            LT::st(sL + f * lstride, idx[e], ln);
+            LT::st(lptr(f, e), 0, ln);
         }
 #pragma unroll
         for (int e = 0; e < d; e += 2) rm[f].set2(e, rn[e], (e + 1 < d) ? rn[e + 1] : 0.0f);
@@ -412,13 +419,47 @@ template <int D, int R, int F, int MODE> struct MsgRegs<D, R, F, MODE, true, fal
     }
 };
 
+// Column offset table (OT layout): for every layer, each thread's byte offsets of its row's columns in
+// a slot's L array, stored as vectors of 4, then 2, then 1 offsets per thread ([chunk][thread]), so a
+// row's offsets arrive in ceil(d/4) or so vector loads and a circulant read needs no index arithmetic.
+__host__ __device__ constexpr int ot_layer_start(int l, int D) { return l < 4 ? QC_DEG_LOW * l : QC_DEG_LOW * 4 + D * (l - 4); }
+
+// Position (in 32-bit words, relative to the layer's region of T * d words) of edge e of thread t.
+__device__ __forceinline__ int ot_pos(int d, int e, int t, int T) {
+    const int c4 = d & ~3, rem = d & 3;
+    if (e < c4) return T * (e & ~3) + 4 * t + (e & 3);
+    if (rem >= 2 && e < c4 + 2) return T * c4 + 2 * t + (e - c4);
+    return T * (c4 + (rem >= 2 ? 2 : 0)) + t;
+}
+
+template <int d, int T>
+__device__ __forceinline__ void ot_load(const uint32_t* tab, int t, int (&idx)[d]) {
+    constexpr int c4 = d & ~3, rem = d & 3;
+#pragma unroll
+    for (int c = 0; c < c4; c += 4) {
+        const uint4 v = reinterpret_cast<const uint4*>(tab + T * c)[t];
+        idx[c] = (int)v.x;
+        idx[c + 1] = (int)v.y;
+        idx[c + 2] = (int)v.z;
+        idx[c + 3] = (int)v.w;
+    }
+    if constexpr (rem >= 2) {
+        const uint2 v = reinterpret_cast<const uint2*>(tab + T * c4)[t];
+        idx[c4] = (int)v.x;
+        idx[c4 + 1] = (int)v.y;
+    }
+    if constexpr (rem & 1) idx[d - 1] = (int)tab[T * (c4 + (rem >= 2 ? 2 : 0)) + t];
+}
+
 // B: resident CTAs per SM the register allocation must allow (0 = the compiler's choice); a larger B
 // caps registers per thread at 65536 / (B * Z/R) and trades registers for resident warps.
 // PAIR: the paired mode above (F = 2, R = 1, 16-bit storage, Approximate-Min*, no clips).
 // RG: messages in global memory (p.r_base, one region of p.slot_elems per slot) instead of
 // registers, for codes whose rows per thread times degrees exceed the register file (K = 16384).
+// OT: the column offset table above, built once per CTA in shared memory after the hard-decision
+// words (T * (12 + 8 D) words); one row per thread.
 template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false,
-          bool RG = false>
+          bool RG = false, bool OT = false>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
@@ -427,6 +468,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     static_assert(!PAIR || (F == 2 && R == 1 && MODE != STORE_FP32 && ALGO == ALGO_AMIN && !CLIP && !RG),
                   "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
     using RE = typename RTraits<MODE>::T;
+    static_assert(!OT || (!PAIR && !RG && R == 1), "the offset table is built for one row per thread");
     using SV = SlotView<MODE, PAIR>;
     using LT = LTraits<MODE>;
     using LE = typename LT::T;
@@ -437,9 +479,11 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const int lstride = (N + 7) & ~7;                      // elements per slot (16-byte multiple)
     LE* sL = reinterpret_cast<LE*>(smem_raw);
     uint32_t* sHB = reinterpret_cast<uint32_t*>(smem_raw + (size_t)F * lstride * sizeof(LE));  // [F][nblk*W]
-    // ALGO_WAMIN: the weight table after the hard-decision words, 16-byte aligned
-    float2* sW = reinterpret_cast<float2*>(
+    // OT: the column offset table after the hard-decision words, 16-byte aligned; ALGO_WAMIN: the
+    // weight table after that
+    uint32_t* sOT = reinterpret_cast<uint32_t*>(
         smem_raw + (((size_t)F * lstride * sizeof(LE) + (size_t)F * (N / 32) * 4 + 15) & ~(size_t)15));
+    float2* sW = reinterpret_cast<float2*>(sOT + (OT ? T * (QC_DEG_LOW * 4 + D * 8) : 0));
     __shared__ uint32_t s_fid[QC_MAX_F];
     __shared__ uint32_t s_sfail[QC_MAX_F];
     __shared__ uint32_t s_be[QC_MAX_F];
@@ -450,6 +494,15 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
 
     MsgRegs<D, R, F, MODE, PAIR, RG> msg;
+    if constexpr (OT) {  // each thread writes and later reads only its own entries: no barrier needed
+        for (int l = 0; l < QC_LAYERS; ++l) {
+            const int d = l < 4 ? QC_DEG_LOW : D;
+            uint32_t* tab = sOT + T * ot_layer_start(l, D);
+            for (int e = 0; e < d; ++e)
+                tab[ot_pos(d, e, tid, T)] =
+                    (uint32_t)((p.blk_off[l][e] + ((tid + p.shift[l][e]) & (Z - 1))) * (int)sizeof(LE));
+        }
+    }
     if constexpr (ALGO == ALGO_WAMIN) {  // visible after the first refill's barrier
         for (int i = tid; i < p.w_iters * p.w_slots; i += T) sW[i] = p.wtab[i];
     }
@@ -552,8 +605,12 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                     const int j = tid + rho * T;
                     if (l < 4) {
                         int idx[QC_DEG_LOW];
+                        if constexpr (OT)
+                            ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(l, D), tid, idx);
+                        else
 #pragma unroll
-                        for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                            for (int e = 0; e < QC_DEG_LOW; ++e)
+                                idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<QC_DEG_LOW, MODE> rm[F];
 #pragma unroll
@@ -565,12 +622,15 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         } else if constexpr (PAIR)
                             row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
                         else
-                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.r3[l & 3][rho], r_cap,
-                                                                       lp_cap, wl);
+                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F, RowMsg<QC_DEG_LOW, MODE>, OT>(
+                                idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap, wl);
                     } else {
                         int idx[D];
+                        if constexpr (OT)
+                            ot_load<D, T>(sOT + T * ot_layer_start(l, D), tid, idx);
+                        else
 #pragma unroll
-                        for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                            for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<D, MODE> rm[F];
 #pragma unroll
@@ -582,8 +642,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         } else if constexpr (PAIR)
                             row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
                         else
-                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap,
-                                                               lp_cap, wl);
+                            row_update<D, MODE, ALGO, CLIP, F, RowMsg<D, MODE>, OT>(
+                                idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap, lp_cap, wl);
                     }
                 }
                 __syncthreads();

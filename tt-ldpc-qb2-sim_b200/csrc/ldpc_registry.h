@@ -8,7 +8,8 @@ namespace ldpcb200 {
 
 struct QcKey {
     int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
-    int G;                                     // 1: messages in global memory (RG kernel)
+    int G;                                     // layout: 0 registers, 1 messages in global memory (RG
+                                               // kernel), 2 registers + column offset table (OT)
     // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
     // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
@@ -42,6 +43,11 @@ const QcTable* qc_tables();
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 1},                                \
      reinterpret_cast<const void*>(                                            \
          &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true>)}
+
+#define LDPC_QC_ENTRY_OT(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                 \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 2},                                \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, false, true>)}
 
 #define LDPC_QC_ENTRY_PAIR(Z, D, MODE, EXT, B)                                 \
     {{Z, D, 1, 2, MODE, ::ldpcb200::ALGO_AMIN, 0, EXT, B, 0},                  \

@@ -39,6 +39,18 @@ static const QcEntry qc_r12k1[] = {
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, true, true),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, false, true),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_NMS, true, true),
+    // column offset table in shared memory (no circulant index arithmetic per edge)
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 5),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 6),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 6),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, true, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, true, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, true, 0),
     // weighted Approximate-Min* (trained weights, LDPC_ALGO_WAMIN): simulation and caller-supplied LLRs
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_WAMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_WAMIN, false, false),
