@@ -326,3 +326,24 @@ def test_weighted_requires_weights_and_rejects_clips(gpu):
         bad[5, 2] = code.n_classes
         with pytest.raises(capi.LdpcError):
             dec.set_weights(np.ones((2, code.n_classes)), np.zeros((2, code.n_classes)), bad)
+
+
+@pytest.mark.parametrize("K,rate,storage", [(1024, "1/2", "fp32"), (1024, "1/2", "fp16"), (4096, "4/5", "fp16"),
+                                            (4096, "4/5", "bf16")])
+def test_weighted_offset_table_shapes_equal_default(gpu, K, rate, storage):
+    code = ar4ja.make_code(K, rate)
+    a, b = _params(code, 20, 3, torch.float32)
+    mu, sigma = capi.channel_mu_sigma(code.N, code.n_checks, code.P, 2.0 if rate == "1/2" else 3.2)
+    with capi.Decoder.from_code(code, 0) as dec:
+        dec.set_weights(a.numpy(), b.numpy(), weighted.edge_class_table(code))
+        p = dec.params(mu=mu, sigma=sigma, seed=5, n_frames=2000 if K == 1024 else 300, max_iter=20,
+                       storage=storage, algo=capi.ALGO_WAMIN)
+        base = dec.run_chunk(p)
+        shapes = [s_ for s_ in dec.shapes(storage, capi.ALGO_WAMIN) if s_[3] == 2]
+        assert shapes
+        for sh in shapes:
+            dec.set_launch_shape(*sh, storage=storage)
+            r = dec.run_chunk(p)
+            dec.set_launch_shape(0, 0, 0, 0, storage=storage)
+            for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters", "bit_errors_sq"):
+                assert getattr(r, k) == getattr(base, k), (sh, k)

@@ -21,5 +21,9 @@ static const QcEntry qc_r23k1[] = {
     LDPC_QC_ENTRY(64, 10, 1, 1, STORE_FP16, ALGO_WAMIN, false, false),
     LDPC_QC_ENTRY(64, 10, 1, 1, STORE_FP16, ALGO_WAMIN, false, true),
     LDPC_QC_ENTRY(64, 10, 1, 1, STORE_FP32, ALGO_WAMIN, false, true),
+    // column offset table in shared memory (layout 2)
+    LDPC_QC_ENTRY_OT(64, 10, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(64, 10, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(64, 10, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
 };
 LDPC_QC_REGISTER(qc_r23k1)

@@ -17,5 +17,9 @@ static const QcEntry qc_r23k4[] = {
     LDPC_QC_ENTRY(256, 10, 1, 1, STORE_BF16, ALGO_AMIN, true, true),
     LDPC_QC_ENTRY(256, 10, 1, 1, STORE_BF16, ALGO_NMS, false, true),
     LDPC_QC_ENTRY(256, 10, 1, 1, STORE_BF16, ALGO_NMS, true, true),
+    // column offset table in shared memory (layout 2)
+    LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
 };
 LDPC_QC_REGISTER(qc_r23k4)

@@ -20,5 +20,8 @@ static const QcEntry qc_r45k1[] = {
     // weighted Approximate-Min* (trained weights, LDPC_ALGO_WAMIN): simulation and caller-supplied LLRs
     LDPC_QC_ENTRY(32, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, false),
     LDPC_QC_ENTRY(32, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, true),
+    // column offset table in shared memory (layout 2)
+    LDPC_QC_ENTRY_OT(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_OT(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
 };
 LDPC_QC_REGISTER(qc_r45k1)
