@@ -535,7 +535,8 @@ def run_mixed(args):
             "l2": "flushed between steps (256 MiB write); inputs generated on chip",
             "codes": {n: {"frames": v["frames"], "fer": v["frame_errors"] / max(v["frames"], 1),
                           "mean_iters": round(v["iters"] / max(v["frames"], 1), 3)} for n, v in per_code.items()},
-            "tuning": {c.name: {"storage": st, "shape": list(sh)} for c, st, sh in zip(wl.codes, wl.storage, wl.shape)},
+            "tuning": {c.name: {"storage": st, "shape": list(sh), "mframes_per_s_alone": round(f / 1e6, 4)}
+                       for c, st, sh, f in zip(wl.codes, wl.storage, wl.shape, wl.rate_fps)},
         },
         "e2e": {"value": round(tot_symbols / e2e_max / 1e9, 4), "unit": UNIT,
                 "h2d_bytes_per_step": int(len(wl.codes) * (wl.decs[0].launch_param_bytes + 64)),
