@@ -433,7 +433,7 @@ __device__ __forceinline__ int ot_pos(int d, int e, int t, int T) {
 }
 
 template <int d, int T>
-__device__ __forceinline__ void ot_load(const uint32_t* tab, int t, int (&idx)[d]) {
+__device__ __forceinline__ void ot_load(const uint32_t* tab, int t, int* idx) {
     constexpr int c4 = d & ~3, rem = d & 3;
 #pragma unroll
     for (int c = 0; c < c4; c += 4) {
@@ -595,6 +595,10 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
 #pragma unroll
             for (int f = 0; f < F; ++f)
                 wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_slots : nullptr;
+            // OT: each layer's offsets are loaded one layer ahead, so their shared-memory latency
+            // overlaps the previous row update
+            int pre[OT ? D : 1];
+            if constexpr (OT) ot_load<QC_DEG_LOW, T>(sOT, tid, pre);
 #pragma unroll
             for (int l = 0; l < QC_LAYERS; ++l) {
                 const float2* wl[F];
@@ -605,9 +609,14 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                     const int j = tid + rho * T;
                     if (l < 4) {
                         int idx[QC_DEG_LOW];
-                        if constexpr (OT)
-                            ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(l, D), tid, idx);
-                        else
+                        if constexpr (OT) {
+#pragma unroll
+                            for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = pre[e];
+                            if (l + 1 < 4)
+                                ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
+                            else
+                                ot_load<D, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
+                        } else
 #pragma unroll
                             for (int e = 0; e < QC_DEG_LOW; ++e)
                                 idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
@@ -626,9 +635,11 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                                 idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap, wl);
                     } else {
                         int idx[D];
-                        if constexpr (OT)
-                            ot_load<D, T>(sOT + T * ot_layer_start(l, D), tid, idx);
-                        else
+                        if constexpr (OT) {
+#pragma unroll
+                            for (int e = 0; e < D; ++e) idx[e] = pre[e];
+                            if (l + 1 < QC_LAYERS) ot_load<D, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
+                        } else
 #pragma unroll
                             for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
                         if constexpr (RG) {
