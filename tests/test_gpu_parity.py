@@ -277,3 +277,23 @@ def test_offset_table_layout_equals_default_on_every_code(gpu, K, rate):
                 for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters",
                           "bit_errors_sq"):
                     assert getattr(r, k) == getattr(base, k), (st, sh, k)
+
+
+@pytest.mark.parametrize("ebn0", [0.0, 2.0, 4.0, 6.0, 8.0])
+def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
+    """With no decoding iterations the tallies count the channel's own hard-decision errors: BPSK
+    over AWGN at Es/N0 = R Eb/N0 must give BER = Q(sqrt(2 R Eb/N0)) (the reference validates its
+    channel the same way, within 1.3 % from 0 to 9 dB).  Here the bar is the 99.9 % interval of the
+    count: the Philox/Box-Muller generator and the mu/sigma scaling (mu = 4 R Eb/N0,
+    sigma = sqrt(8 R Eb/N0)) together."""
+    from scipy import stats
+    c = ar4ja.make_code(1024, "1/2")
+    R = (c.N - c.n_checks) / (c.N - c.P)
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, ebn0)
+    frames = 1 << 17
+    r = dec_r12k1.run_chunk(dec_r12k1.params(mu=mu, sigma=sigma, seed=21, n_frames=frames, max_iter=0, storage="fp32"))
+    assert r.iter_sum == 0 and r.frames == frames
+    bits = frames * c.n_tx
+    p = float(stats.norm.sf(np.sqrt(2.0 * R * 10.0 ** (ebn0 / 10.0))))
+    lo, hi = stats.binom.interval(0.999, bits, p)
+    assert lo <= r.bit_errors <= hi, (ebn0, r.bit_errors / bits, p)
