@@ -147,21 +147,26 @@ def test_float64_adjoint_matches_central_differences(gpu):
     assert (got[m] - central[m]).norm().item() <= 1e-3 * central[m].norm().item()
 
 
-def test_float64_adjoint_matches_torch_autograd(gpu):
-    code = ar4ja.make_code(1024, "4/5")
-    T, B = 10, 16
-    llr = _llr(code, B, 2.5, 23, np.float64)
+@pytest.mark.parametrize("K,rate,T,B,post_all", [(1024, "1/2", 20, 64, True), (1024, "4/5", 10, 16, False)])
+def test_float64_adjoint_matches_torch_autograd(gpu, K, rate, T, B, post_all):
+    """The hand-written float64 adjoint against plain-PyTorch autograd of the same decoder: the
+    training configuration (rate 1/2, T = 20, 64 frames, checkpoints every 5 iterations, all
+    posteriors) and a rate-4/5 one (degree 18 rows, last posterior only, checkpoints every 4)."""
+    code = ar4ja.make_code(K, rate)
+    llr = _llr(code, B, 1.5 if rate == "1/2" else 2.5, 23, np.float64)
     a, b = _params(code, T, 4)
-    gpost = torch.randn(1, B, code.N, generator=torch.Generator().manual_seed(8), dtype=torch.float64)
+    gpost = torch.randn(T if post_all else 1, B, code.N, generator=torch.Generator().manual_seed(8),
+                        dtype=torch.float64)
     with capi.Decoder.from_code(code, 0) as dec:
-        post, (gx, ga, gb) = _run(code, dec, llr, a, b, T, ckpt=4, post_all=False, want_grad=True, gpost=gpost)
-    x = torch.from_numpy(llr).requires_grad_()
-    ar, br = a.clone().requires_grad_(), b.clone().requires_grad_()
-    pr = wref.decode(code, x, ar, br, post_all=False)
-    assert torch.allclose(post.cpu(), pr.detach(), rtol=1e-12, atol=1e-9)
-    pr.backward(gpost)
+        post, (gx, ga, gb) = _run(code, dec, llr, a, b, T, ckpt=5 if post_all else 4, post_all=post_all,
+                                  want_grad=True, gpost=gpost)
+    x = torch.from_numpy(llr).to(DEV).requires_grad_()
+    ar, br = a.to(DEV).requires_grad_(), b.to(DEV).requires_grad_()
+    pr = wref.decode(code, x, ar, br, post_all=post_all)
+    assert torch.allclose(post, pr.detach(), rtol=1e-12, atol=1e-9)
+    pr.backward(gpost.to(DEV))
     for got, ref in ((ga, ar.grad), (gb, br.grad), (gx, x.grad)):
-        assert torch.allclose(got.cpu(), ref, rtol=1e-9, atol=1e-9 * max(1.0, ref.abs().max().item()))
+        assert torch.allclose(got, ref, rtol=1e-9, atol=1e-9 * max(1.0, ref.abs().max().item()))
 
 
 def test_gradients_do_not_depend_on_checkpoint_interval(gpu):
