@@ -1,5 +1,4 @@
 """Matrix-file parsing: formats and error behaviour of ldpc_sim_scalar.cpp:116-269."""
-import numpy as np
 import pytest
 
 from ldpcb200 import ar4ja, chinn

@@ -11,7 +11,7 @@ import sys
 import pytest
 import torch.multiprocessing as mp
 
-from conftest import REPO, SRC
+from conftest import SRC
 
 
 def stand_in(first, n):

@@ -17,7 +17,6 @@ end at most the reference interval's upper end); in the waterfall it is measurab
 import json
 import os
 
-import numpy as np
 import pytest
 
 from conftest import REPO, golden_matrix

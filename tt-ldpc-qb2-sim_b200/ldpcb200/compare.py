@@ -24,7 +24,6 @@ import sys
 import time
 from typing import Dict, List, Optional, Sequence, Tuple
 
-import numpy as np
 
 from . import ar4ja, capi, weighted
 from .stats import ber_interval, clopper_pearson, intervals_overlap

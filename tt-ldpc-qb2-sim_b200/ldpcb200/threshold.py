@@ -14,7 +14,6 @@ rate), not on the lifting size K.
 """
 from __future__ import annotations
 
-import math
 from functools import lru_cache
 from typing import Dict
 
