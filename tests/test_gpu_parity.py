@@ -297,3 +297,31 @@ def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
     p = float(stats.norm.sf(np.sqrt(2.0 * R * 10.0 ** (ebn0 / 10.0))))
     lo, hi = stats.binom.interval(0.999, bits, p)
     assert lo <= r.bit_errors <= hi, (ebn0, r.bit_errors / bits, p)
+
+
+def test_sim_cli_long_run_picks_a_shape_and_keeps_the_tallies(tmp_path):
+    """The drop-in binary's engine times the built launch shapes before a long run (2^22 frames) and
+    reports the choice; the tallies equal a run with the default shape (shapes change only speed)."""
+    import io
+    import json
+    from ldpcb200 import sim
+    c = ar4ja.make_code(1024, "1/2")
+    m = tmp_path / "r12k1.chinn.out"
+    m.write_text(c.chinn_out_text())
+    args = ["-c", str(m), "-e", "2.0", "-p", "512", "-s", "-k", str(1 << 22), "-m", str(1 << 22),
+            "-b", str(1 << 21), "-i", "200", "-t", "1000000000", "--storage", "fp32", "--seed", "3"]
+    out = io.StringIO()
+    assert sim.main(args, out=out) == 0
+    text = out.getvalue()
+    assert "[CONFIG] Launch shape" in text
+    final = json.loads(text.strip().splitlines()[-1])
+    assert final["blocks"] == 1 << 22
+    with capi.Decoder.from_code(c, 0) as dec:
+        mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 2.0)
+        tot = [0, 0]
+        for first in (0, 1 << 21):
+            r = dec.run_chunk(dec.params(mu=mu, sigma=sigma, seed=3, first_frame=first, n_frames=1 << 21,
+                                         max_iter=200, storage="fp32"))
+            tot[0] += r.bit_errors
+            tot[1] += r.frame_errors
+    assert [final["bit_errors"], final["frame_errors"]] == tot

@@ -134,6 +134,17 @@ class GpuEngine:
     def describe(self) -> str:
         return "layered QC kernel" if self.dec.kind == self.capi.KERNEL_QC else "general file-order kernel"
 
+    def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
+        """For long runs of the QC kernel (plain Approximate-Min*, no clips), time every built launch
+        shape of the chosen storage on 2^16 frames of this channel (another seed) and keep the
+        fastest.  Shapes change only the speed: every shape decodes every frame to the same bits."""
+        if (self.dec.kind != self.capi.KERNEL_QC or o.nms or o.r_max > 0 or o.l_post_max > 0 or o.l_max > 0
+                or o.gamma > 0 or max_blocks < TUNE_MIN_BLOCKS):
+            return None
+        res, _ = self.dec.autotune(mu, sigma, storages=(o.storage,), frames=1 << 16, max_iter=o.max_iter,
+                                   repeats=1)
+        return res.get(o.storage, (None,))[0]
+
     def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
         p = self.dec.params(mu=mu, sigma=sigma, seed=o.seed, first_frame=first, n_frames=n,
                             max_iter=o.max_iter, storage=o.storage,
@@ -144,6 +155,9 @@ class GpuEngine:
 
     def close(self):
         self.dec.close()
+
+
+TUNE_MIN_BLOCKS = 1 << 22  # runs at least this long pick their launch shape first
 
 
 def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = None, out=None) -> int:
@@ -202,6 +216,12 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
     elif l_max > 0 or o.r_max > 0 or o.l_post_max > 0:
         say(f"[CONFIG] LLR Clipping (Fixed): L_ch_max={_g(l_max)}, R_max={_g(o.r_max)}, "
             f"L_post_max={_g(o.l_post_max)}")
+
+    if hasattr(engine, "tune"):
+        shape = engine.tune(o, mu, sigma, max_blocks)
+        if shape is not None:
+            say(f"[CONFIG] Launch shape {','.join(map(str, shape))} (rows/thread, frames/CTA, CTAs/SM cap, "
+                f"layout), the fastest of the built shapes on this channel")
 
     blocks = be = fe = iters = 0
     kernel_ms = 0.0
