@@ -767,18 +767,7 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
     CU(cudaGraphCreate(&g, 0));
     int rc = 0;
     int64_t kernels = 0;
-    // kernels enter the graph largest first (frames x edges per frame): with full grids the block
-    // scheduler starts each kernel's CTAs as earlier ones retire, so the short kernels fill the long
-    // ones' tails (longest-processing-time-first order)
-    std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    auto work = [&](int i) {
-        const ldpc_handle* h = b->hs[i];
-        return (double)params[i].n_frames * h->Z * (4 * QC_DEG_LOW + 8 * h->D);
-    };
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
-    for (int oi = 0; oi < n && !rc; ++oi) {
-        const int i = order[oi];
+    for (int i = 0; i < n && !rc; ++i) {
         ldpc_handle* h = b->hs[i];
         cudaGraphNode_t deps[4];
         if ((rc = add_memset(g, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), &deps[0])) ||
