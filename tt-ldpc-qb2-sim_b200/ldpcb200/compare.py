@@ -4,6 +4,7 @@ For each code and Eb/N0 point, the plain Approximate-Min* decoder (at most 200 i
 weighted decoder with its trained weights (capped at T iterations, one decoder per cap) decode the
 SAME frames -- the channel of a frame depends only on (seed, stream, frame index) -- as kernels of
 one CUDA-graph launch per chunk (the batched path), so the error counts are a paired comparison.
+Controls: the plain decoder capped at the same T (what the weights add beyond the cap).
 A point runs until ``--frames`` frames or until every decoder has ``--min-errors`` frame errors.  Each
 decoder's GPU time per decoded frame is then measured on its own (one persistent kernel, CUDA
 events) on a sample of the same frames.  Every decoder runs in the message storage and launch shape
@@ -52,7 +53,7 @@ def _tune(dec: capi.Decoder, code: ar4ja.QcCode, ebn0: float, max_iter: int, alg
 
 def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps: Sequence[int],
                  time_frames: int, device: int = 0, log=print, min_errors: int = 1000,
-                 weights: Optional[str] = None) -> dict:
+                 weights: Optional[str] = None, controls: bool = True) -> dict:
     decs: List[capi.Decoder] = []
     names: List[str] = []
     iters: List[int] = []
@@ -74,6 +75,11 @@ def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps:
             decs.append(d); names.append(f"weighted_t{cap}"); iters.append(cap)
             algos.append(capi.ALGO_WAMIN); storages.append(st)
             wsrc[names[-1]] = src
+            if controls:  # the plain decoder with the same cap: what the weights add beyond the cap
+                d = capi.Decoder.from_code(code, device)
+                st, _ = _tune(d, code, mid, cap, capi.ALGO_AMIN, tune_frames)
+                decs.append(d); names.append(f"plain_t{cap}"); iters.append(cap)
+                algos.append(capi.ALGO_AMIN); storages.append(st)
         batch = capi.Batch(decs)
         out = {"code": code.name, "n_tx": code.n_tx, "frames_per_point": frames, "weights": wsrc,
                "storage": dict(zip(names, storages)), "points": {}}
@@ -121,11 +127,15 @@ def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps:
                 dd = pt["decoders"][name]
                 dd["fer_matches_plain"] = intervals_overlap(tuple(dd["fer_ci95"]), tuple(base["fer_ci95"]))
                 dd["time_ratio_vs_plain"] = dd["gpu_us_per_frame"] / base["gpu_us_per_frame"]
+                ctl = pt["decoders"].get(name.replace("weighted_", "plain_"))
+                if name.startswith("weighted_") and ctl is not None:
+                    dd["fer_vs_plain_same_cap"] = dd["fer"] / ctl["fer"] if ctl["fer"] > 0 else None
             out["points"][str(eb)] = pt
             log(json.dumps({"code": code.name, "ebn0": eb, **{n: {k: (round(v, 6) if isinstance(v, float) else v)
                                                                   for k, v in d_.items() if k in (
                                                                       "fer", "mean_iters", "gpu_us_per_frame",
-                                                                      "fer_matches_plain", "time_ratio_vs_plain")}
+                                                                      "fer_matches_plain", "time_ratio_vs_plain",
+                                                                      "fer_vs_plain_same_cap")}
                                                               for n, d_ in pt["decoders"].items()}}))
         batch.close()
         return out
@@ -145,6 +155,7 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
                     help="stop a point once every decoder has this many frame errors")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--weights", default="", help="weights file to use instead of the committed ones")
+    ap.add_argument("--no-controls", action="store_true", help="skip the plain decoders capped at each T")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     results = []
@@ -153,7 +164,7 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
         code = ar4ja.make_code(int(K), rate)
         results.append(compare_code(code, a.ebn0, a.frames, a.caps, a.time_frames, a.device,
                                     log=lambda s: print(s, flush=True), min_errors=a.min_errors,
-                                    weights=a.weights or None))
+                                    weights=a.weights or None, controls=not a.no_controls))
     doc = {"seed": SEED, "plain_max_iter": PLAIN_ITERS, "caps": a.caps, "max_frames_per_point": a.frames,
            "min_errors": a.min_errors, "results": results}
     if a.out:
