@@ -230,6 +230,158 @@ int oracle_decode_nostop(int N, int M, int P, int dmax, const int32_t* rows, con
                        post, r_work, iters, synd_fail, bit_errors, 0);
 }
 
+/* ---------------- the circulant engine's decoder (rate 1/2 AR4JA, degrees 3 and 6) ---------------- */
+
+/*
+ * Restates the check-node arithmetic of the reference's circulant-engine golden stepper
+ * (tests/test_circulant_dma_stepper.cpp) in its two forms:
+ *
+ *   CIRC_SCALAR  step_tile_circulant_dma_scalar (:332-482) with approx_min_star (:39-54): q = L - r
+ *                in fp32, exact correction constants, r = +-mag, L = store(q + r) with r unrounded;
+ *   CIRC_SFPU    step_tile_circulant_dma_sfpu (:487-565) with compute_tile_deg6_sfpi (:110-273) /
+ *                compute_tile_deg3_sfpi (:278-327) and sfpi_amin_star_branchless
+ *                (engines/tile_matrix_4cw/sfpi_host_emu.h:590-607), the device engine's math
+ *                (engines/circulant_dma_4cw/compute_trisc.cpp:75-96, 299-658): Q = store(L - r), the
+ *                correction constants truncated to bf16, mag scaled by the damping factor,
+ *                r = store(+-mag), L = store(Q + r).
+ *
+ * Both use the min* g(a, b) = max(min(a, b) - max(c1 + k1 |a-b|, c2 + k2 |a-b|, 0), 0) with
+ * (c1, k1, c2, k2) = (0.69315, -0.4, 0.65715, -0.328), and the pairwise tree of the degree-6 rows:
+ * m03 = g(a0, a3), m14 = g(a1, a4), m25 = g(a2, a5); edge 0 gets g(g(m14, m25), a3), edge 3
+ * g(g(m14, m25), a0), and likewise for the pairs (1, 4) and (2, 5); a degree-3 row gives each edge
+ * g of the other two.  Edges are a row's columns in ascending order (the descriptor tables' edge
+ * index, tools/generate_circulant_dma_tables.py:153-185).  Rows are visited in the order given
+ * (the engine's tile schedule: rows 512..1535, then 0..511 for K = 1024).
+ *
+ * Stop and tally:
+ *   CIRC_STOP_SYNDROME  the stepper's Monte Carlo loop (tests/test_circulant_dma_stepper.cpp:773-822):
+ *                       full syndrome after every iteration (bit = value < 0); a frame that never
+ *                       meets it is a frame error with bit errors = info positions with value <= 0;
+ *   CIRC_STOP_GENIE     the device engine (engines/circulant_dma_4cw/reader_brisc.cpp:166-198,
+ *                       writer_ncrisc.cpp:265-337): stop once no info position has its sign bit
+ *                       set; a frame that never stops is a frame error with bit errors = info
+ *                       positions with the sign bit set.
+ * A frame that stops reports zero bit errors, as both do.
+ */
+#define CIRC_SCALAR 0
+#define CIRC_SFPU 1
+#define CIRC_STOP_SYNDROME 0
+#define CIRC_STOP_GENIE 1
+
+static inline float trunc_bf16(float x) { return u2f(f2u(x) & 0xFFFF0000u); }
+
+typedef struct { float c1, k1, c2, k2; } circ_consts;
+
+static inline float circ_g(const circ_consts* k, float a, float b) {
+    float mn = (b < a) ? b : a;
+    float mx = (a < b) ? b : a;
+    float diff = mx - mn;
+    float line1 = k->c1 + k->k1 * diff;
+    float line2 = k->c2 + k->k2 * diff;
+    float corr = (line1 < line2) ? line2 : line1;
+    if (corr < 0.0f) corr = 0.0f;
+    float v = mn - corr;
+    return (v < 0.0f) ? 0.0f : v;
+}
+
+static int syndrome_failures_lt0(int M, int dmax, const int32_t* rows, const int32_t* degs, const float* L) {
+    int fails = 0;
+    for (int m = 0; m < M; m++) {
+        int par = 0;
+        for (int d = 0; d < degs[m]; d++) par ^= (L[rows[(size_t)m * dmax + d]] < 0.0f);
+        fails += par;
+    }
+    return fails;
+}
+
+/*
+ * order [M]: the rows in update order.  n_info: the info positions 0..n_info-1 of the tally.
+ * Outputs: post [N] final L, *iters, *synd_fail (rows failing, sign-bit parity), *bit_errors and
+ * *frame_error as the engine tallies them.  Returns 0, or -1 on bad arguments (a row degree other
+ * than 3 or 6, damping outside (0, 1]).
+ */
+int oracle_circ_decode(int N, int M, int P, int dmax, const int32_t* rows, const int32_t* degs,
+                       const int32_t* order, int n_info, int mode, int numerics, float damping, int stop,
+                       int max_iter, const float* llr_tx, float* post, float* r_work, int32_t* iters,
+                       int32_t* synd_fail, int32_t* bit_errors, int32_t* frame_error) {
+    if (N <= 0 || M <= 0 || P < 0 || P > N || dmax < 3 || dmax > ORC_MAX_DEG || n_info < 0 || n_info > N)
+        return -1;
+    if (!(damping > 0.0f && damping <= 1.0f)) return -1;
+    for (int m = 0; m < M; m++)
+        if (degs[m] != 3 && degs[m] != 6) return -1;
+    circ_consts k = {0.69315f, -0.40f, 0.65715f, -0.328f};
+    if (numerics == CIRC_SFPU) {
+        k.c1 = trunc_bf16(k.c1); k.k1 = trunc_bf16(k.k1);
+        k.c2 = trunc_bf16(k.c2); k.k2 = trunc_bf16(k.k2);
+    }
+    const int ntx = N - P;
+    float* L = post;
+    for (int i = 0; i < ntx; i++) L[i] = store_L(mode, llr_tx[i]);
+    for (int i = ntx; i < N; i++) L[i] = 0.0f;
+    float* r = r_work;
+    for (size_t i = 0; i < (size_t)M * dmax; i++) r[i] = 0.0f;
+
+    int stopped = 0, it_used = max_iter;
+    for (int it = 0; it < max_iter && !stopped; it++) {
+        for (int oi = 0; oi < M; oi++) {
+            const int m = order[oi];
+            const int deg = degs[m];
+            const int32_t* vn = rows + (size_t)m * dmax;
+            float* rm = r + (size_t)m * dmax;
+            float q[6], a[6], mag[6];
+            uint32_t par = 0, neg[6];
+            for (int d = 0; d < deg; d++) {
+                q[d] = L[vn[d]] - rm[d];
+                if (numerics == CIRC_SFPU) {
+                    q[d] = store_L(mode, q[d]);
+                    neg[d] = f2u(q[d]) >> 31;          /* sign bit (sfpi::as<vInt> XOR) */
+                } else {
+                    neg[d] = q[d] < 0.0f;              /* (q < 0) ? -1 : 1 */
+                }
+                par ^= neg[d];
+                a[d] = fabs_bits(q[d]);
+            }
+            if (deg == 6) {
+                float m03 = circ_g(&k, a[0], a[3]), m14 = circ_g(&k, a[1], a[4]), m25 = circ_g(&k, a[2], a[5]);
+                float o0 = circ_g(&k, m14, m25), o1 = circ_g(&k, m03, m25), o2 = circ_g(&k, m03, m14);
+                mag[0] = circ_g(&k, o0, a[3]); mag[3] = circ_g(&k, o0, a[0]);
+                mag[1] = circ_g(&k, o1, a[4]); mag[4] = circ_g(&k, o1, a[1]);
+                mag[2] = circ_g(&k, o2, a[5]); mag[5] = circ_g(&k, o2, a[2]);
+            } else {
+                mag[0] = circ_g(&k, a[1], a[2]);
+                mag[1] = circ_g(&k, a[0], a[2]);
+                mag[2] = circ_g(&k, a[0], a[1]);
+            }
+            for (int d = 0; d < deg; d++) {
+                float mg = mag[d];
+                /* the degree-6 kernel always multiplies, the degree-3 one only below 1 (x 1 is exact) */
+                if (numerics == CIRC_SFPU) mg = mg * damping;
+                float rn = u2f(f2u(mg) | ((par ^ neg[d]) << 31));
+                float rs = store_r(mode, rn);
+                L[vn[d]] = store_L(mode, q[d] + (numerics == CIRC_SFPU ? rs : rn));
+                rm[d] = rs;
+            }
+        }
+        if (stop == CIRC_STOP_GENIE) {
+            int errs = 0;
+            for (int i = 0; i < n_info; i++) errs += (int)(f2u(L[i]) >> 31);
+            if (errs == 0) { stopped = 1; it_used = it + 1; }
+        } else if (syndrome_failures_lt0(M, dmax, rows, degs, L) == 0) {
+            stopped = 1;
+            it_used = it + 1;
+        }
+    }
+    *iters = it_used;
+    *synd_fail = syndrome_failures(M, dmax, rows, degs, L);
+    int be = 0;
+    if (!stopped)
+        for (int i = 0; i < n_info; i++)
+            be += stop == CIRC_STOP_GENIE ? (int)(f2u(L[i]) >> 31) : (L[i] <= 0.0f);
+    *bit_errors = be;
+    *frame_error = !stopped;
+    return 0;
+}
+
 /* ---------------- the reference's channel: xoshiro128+ and the polar method ---------------- */
 
 typedef struct { uint32_t s[4]; } xo128;

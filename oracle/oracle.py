@@ -22,6 +22,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 STORE_BF16, STORE_FP32, STORE_FP16 = 0, 1, 2
 ALGO_AMIN, ALGO_NMS = 0, 1
+CIRC_SCALAR, CIRC_SFPU = 0, 1
+CIRC_STOP_SYNDROME, CIRC_STOP_GENIE = 0, 1
 
 _lib = None
 
@@ -56,6 +58,11 @@ def lib():
         L.oracle_mc_pairs.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int32), P(C.c_int32),
                                       C.c_int, C.c_float, C.c_float, P(C.c_uint32), C.c_int,
                                       P(C.c_float), P(C.c_uint64)]
+        L.oracle_circ_decode.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int32), P(C.c_int32),
+                                         P(C.c_int32), C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                         C.c_int, P(C.c_float), P(C.c_float), P(C.c_float),
+                                         P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int32)]
+        L.oracle_circ_decode.restype = C.c_int
         _lib = L
     return _lib
 
@@ -109,6 +116,39 @@ def decode(code: Code, llr: np.ndarray, mode: int = STORE_BF16, algo: int = ALGO
             raise ValueError("oracle_decode rejected its arguments")
         iters[i], sf[i], be[i] = it.value, s.value, b.value
     return post, iters, sf, be
+
+
+def circ_schedule(code: Code) -> np.ndarray:
+    """The circulant engine's row order: the degree-6 rows in index order, then the degree-3 rows
+    (engines/circulant_dma_4cw/ar4ja_circulant_descriptors_4cw.h:29-31, tiles 0-31 then 32-39)."""
+    idx = np.arange(code.M, dtype=np.int32)
+    return np.ascontiguousarray(np.concatenate([idx[code.degs != 3], idx[code.degs == 3]]), dtype=np.int32)
+
+
+def circ_decode(code: Code, llr: np.ndarray, numerics: int = CIRC_SFPU, damping: float = 1.0,
+                stop: int = CIRC_STOP_SYNDROME, max_iter: int = 200, mode: int = STORE_BF16,
+                n_info: Optional[int] = None, order: Optional[np.ndarray] = None):
+    """The circulant engine's decoder (``oracle_circ_decode``) on frames ``llr`` [n, N-P].  Returns
+    (post [n, N], iters, synd_fail, bit_errors, frame_error); bit errors and frame errors as that
+    engine tallies them (over the info positions 0..n_info-1, default N - M)."""
+    L = lib()
+    llr = np.ascontiguousarray(np.atleast_2d(llr), dtype=np.float32)
+    n = llr.shape[0]
+    order = circ_schedule(code) if order is None else np.ascontiguousarray(order, dtype=np.int32)
+    n_info = code.N - code.M if n_info is None else int(n_info)
+    post = np.zeros((n, code.N), dtype=np.float32)
+    rw = np.zeros(code.M * code.dmax, dtype=np.float32)
+    out = np.zeros((4, n), np.int32)
+    for i in range(n):
+        v = [C.c_int32() for _ in range(4)]
+        rc = L.oracle_circ_decode(code.N, code.M, code.P, code.dmax, _p(code.rows, C.c_int32),
+                                  _p(code.degs, C.c_int32), _p(order, C.c_int32), n_info, mode, numerics,
+                                  damping, stop, max_iter, _p(llr[i], C.c_float), _p(post[i], C.c_float),
+                                  _p(rw, C.c_float), *[C.byref(x) for x in v])
+        if rc != 0:
+            raise ValueError("oracle_circ_decode rejected its arguments")
+        out[:, i] = [x.value for x in v]
+    return post, out[0], out[1], out[2], out[3]
 
 
 def philox4x32_10(ctr, key) -> np.ndarray:
@@ -219,3 +259,41 @@ def run_ref_mc(code: Code, mu: float, sigma: float, max_iter: int, max_frames: i
                             str(max_iter), str(max_frames), str(budget_s), str(seed), str(threads)],
                            check=True, capture_output=True, text=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_ref_circ(llr_bf16_bits: np.ndarray, sfpu: bool, damping: float, max_iter: int):
+    """The reference's circulant golden stepper (oracle/_ref/ref_circ) on codewords of AR4JA r1/2
+    K = 1024: llr_bf16_bits [n, 2048] u16 channel LLRs as bf16 bits, n a multiple of 4.  Returns
+    (post bits [n, 2560] u16, iters [n], active [n], bit_errors [n])."""
+    exe = ref_binary("ref_circ")
+    if exe is None:
+        raise FileNotFoundError("oracle/_ref/ref_circ is not built (make -C oracle ref)")
+    x = np.asarray(llr_bf16_bits, dtype=np.uint16)
+    n = x.shape[0]
+    assert n % 4 == 0 and x.shape[1] == 2048
+    groups = n // 4
+    nodes = np.zeros((groups, 2560, 4), np.uint16)
+    nodes[:, :2048, :] = x.reshape(groups, 4, 2048).transpose(0, 2, 1)
+    with tempfile.TemporaryDirectory() as td:
+        ip = os.path.join(td, "in.bin")
+        op = os.path.join(td, "out.bin")
+        with open(ip, "wb") as f:
+            f.write(np.uint32(groups).tobytes())
+            f.write(nodes.tobytes())
+        subprocess.run([exe, ip, op, "1" if sfpu else "0", repr(float(np.float32(damping))), str(max_iter)],
+                       check=True)
+        raw = np.fromfile(op, dtype=np.uint8)
+    per = 2560 * 8 + 3 * 16
+    assert raw.size == groups * per
+    post = np.zeros((n, 2560), np.uint16)
+    iters = np.zeros(n, np.int64)
+    active = np.zeros(n, np.int64)
+    be = np.zeros(n, np.int64)
+    for g in range(groups):
+        blk = raw[g * per:(g + 1) * per]
+        post[4 * g:4 * g + 4] = blk[:2560 * 8].view(np.uint16).reshape(2560, 4).T
+        tail = blk[2560 * 8:].view(np.uint32)
+        iters[4 * g:4 * g + 4] = tail[0:4]
+        active[4 * g:4 * g + 4] = tail[4:8]
+        be[4 * g:4 * g + 4] = tail[8:12]
+    return post, iters, active, be

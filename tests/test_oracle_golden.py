@@ -76,3 +76,99 @@ def test_fp16_rounding_is_ieee():
     x = np.array([1e-8, 6.1e-5, 3.0001, 65519.0, 70000.0, -2.5e-6], np.float32)
     sat = np.clip(x, -65504, 65504).astype(np.float16).astype(np.float32)
     assert sat[3] == 65504.0 and sat[4] == 65504.0
+
+
+# ----------------------------- the circulant engine's decoder -----------------------------
+
+def _circ_golden():
+    import os
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_circulant_stepper.npz")
+    return np.load(p)
+
+
+def _r12k1_code():
+    from ldpcb200 import ar4ja
+    c = ar4ja.make_code(1024, "1/2")
+    return O.Code(c.row_matrix(), c.N, c.P)
+
+
+def _bits_to_f32(bits):
+    return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def _f32_to_bf16_bits(x):
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+@pytest.mark.parametrize("idx", range(7))
+def test_circ_oracle_matches_reference_stepper(idx):
+    """oracle_circ_decode against the reference's circulant golden stepper
+    (tests/test_circulant_dma_stepper.cpp, scalar and SFPU-emulated paths, its Monte Carlo loop's
+    syndrome stop and tally): the same bf16 nodes, iterations, frame errors and bit errors."""
+    z = _circ_golden()
+    code = _r12k1_code()
+    llr = _bits_to_f32(z["llr_bits"][idx])
+    post, it, sf, be, fe = O.circ_decode(code, llr, numerics=O.CIRC_SFPU if z["sfpu"][idx] else O.CIRC_SCALAR,
+                                         damping=float(z["damping"][idx]), stop=O.CIRC_STOP_SYNDROME,
+                                         max_iter=int(z["max_iter"][idx]))
+    assert np.array_equal(_f32_to_bf16_bits(post), z["post_bits"][idx])
+    assert np.array_equal(post.view(np.uint32) & 0xFFFF, np.zeros_like(post.view(np.uint32)))  # bf16 values
+    assert np.array_equal(it, z["iters"][idx])
+    assert np.array_equal(fe, z["frame_error"][idx])
+    assert np.array_equal(be, z["bit_errors"][idx])
+    # a frame that met the syndrome has no failing rows
+    assert (sf[fe == 0] == 0).all()
+
+
+def test_circ_oracle_matches_reference_stepper_live():
+    """The same against the reference stepper binary itself on fresh frames (when oracle/_ref is
+    built from the reference's sources)."""
+    if O.ref_binary("ref_circ") is None:
+        pytest.skip("reference binaries not built")
+    code = _r12k1_code()
+    rng = np.random.default_rng(77)
+    for eb, sfpu, damp, mi in ((0.75, False, 1.0, 30), (1.25, True, 0.9375, 30), (2.0, True, 0.8, 8)):
+        g = 10.0 ** (eb / 10.0)
+        bits = _f32_to_bf16_bits(2.0 * g + np.sqrt(4.0 * g) * rng.standard_normal((16, 2048)))
+        pr, ir, ar, br = O.run_ref_circ(bits, sfpu, damp, mi)
+        post, it, sf, be, fe = O.circ_decode(code, _bits_to_f32(bits), numerics=int(sfpu), damping=damp,
+                                             max_iter=mi)
+        assert np.array_equal(_f32_to_bf16_bits(post), pr)
+        assert np.array_equal(it, ir) and np.array_equal(fe, ar) and np.array_equal(be, br)
+
+
+def test_circ_genie_stop_and_tally():
+    """The device engine's stop (no info sign bit set) ends a frame no later than the syndrome stop
+    on frames that decode to the all-zero codeword, and both report zero bit errors for stopped
+    frames; an unstopped frame's bit errors are its info sign bits."""
+    code = _r12k1_code()
+    rng = np.random.default_rng(5)
+    llr = _bits_to_f32(_f32_to_bf16_bits(3.2 + 2.53 * rng.standard_normal((12, 2048))))  # 2 dB
+    _, it_s, _, be_s, fe_s = O.circ_decode(code, llr, numerics=O.CIRC_SFPU, damping=0.9375,
+                                           stop=O.CIRC_STOP_SYNDROME, max_iter=100)
+    post, it_g, _, be_g, fe_g = O.circ_decode(code, llr, numerics=O.CIRC_SFPU, damping=0.9375,
+                                              stop=O.CIRC_STOP_GENIE, max_iter=100)
+    ok = fe_s == 0
+    assert ok.sum() >= 10
+    assert (it_g[ok] <= it_s[ok]).all()
+    assert (be_g[fe_g == 0] == 0).all() and (be_s[ok] == 0).all()
+    _, it1, _, be1, fe1 = O.circ_decode(code, llr, numerics=O.CIRC_SFPU, damping=0.9375,
+                                        stop=O.CIRC_STOP_GENIE, max_iter=1)
+    post1, *_ = O.circ_decode(code, llr, numerics=O.CIRC_SFPU, damping=0.9375, stop=O.CIRC_STOP_GENIE,
+                              max_iter=1)
+    signs = (post1[:, :1024].view(np.uint32) >> 31).sum(axis=1)
+    assert np.array_equal(be1, np.where(fe1 == 1, signs, 0))
+    assert np.array_equal(fe1, (signs > 0).astype(np.int32))
+
+
+def test_circ_oracle_rejects_bad_arguments():
+    from ldpcb200 import ar4ja
+    c = ar4ja.make_code(1024, "2/3")  # degree-10 rows: no pairwise tree
+    code = O.Code(c.row_matrix(), c.N, c.P)
+    with pytest.raises(ValueError):
+        O.circ_decode(code, np.zeros((1, c.n_tx), np.float32), max_iter=1)
+    code12 = _r12k1_code()
+    for damp in (0.0, 1.5, float("nan")):
+        with pytest.raises(ValueError):
+            O.circ_decode(code12, np.zeros((1, 2048), np.float32), damping=damp, max_iter=1)
