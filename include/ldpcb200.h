@@ -44,6 +44,7 @@ extern "C" {
 #define LDPC_ALGO_AMIN 0 /* Approximate-Min* (Jones, MILCOM 2003) */
 #define LDPC_ALGO_NMS 1  /* normalised min-sum, alpha = 0.75 */
 #define LDPC_ALGO_WAMIN 2 /* weighted Approximate-Min* with the handle's weights (ldpc_set_weights) */
+#define LDPC_ALGO_CIRC 3  /* the circulant engine's decoder with the handle's settings (ldpc_set_circulant) */
 
 /* Decoder family chosen for a matrix (ldpc_kernel_kind). */
 #define LDPC_KERNEL_QC 0      /* quasi-cyclic layered kernel (AR4JA structure detected) */
@@ -200,6 +201,38 @@ int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const
  * n_iter = 0 removes the weights.  QC codes only; no clips.  No counterpart in the reference. */
 int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float* beta, int n_iter, int n_classes,
                      const int32_t* edge_class);
+
+/* The circulant engine's decoder for LDPC_ALGO_CIRC runs of this handle: the check-node arithmetic
+ * of engines/circulant_dma_4cw/compute_trisc.cpp:299-658 as its golden stepper states it
+ * (tests/test_circulant_dma_stepper.cpp:39-565, run_monte_carlo :708-822).  Replaces the
+ * per-invocation settings of ldpc_sim_circulant_dma.cpp:526-572 and of the stepper's command line.
+ *   - rows of degree 3 and 6 only (the rate-1/2 AR4JA codes), degree-6 layers first (the engine's
+ *     tile schedule: rows 512..1535, then 0..511, for K = 1024), edges in ascending column order;
+ *   - degree-6 magnitudes from the pairwise min* tree (pairs (0,3), (1,4), (2,5)), degree 3 from the
+ *     other two edges; min* g = max(min - max(c1 - 0.4 d, c2 - 0.328 d, 0), 0), c1 = 0.69315,
+ *     c2 = 0.65715 (not the scalar engine's piecewise form);
+ *   - numerics LDPC_CIRC_SFPU: the SFPU kernel (constants truncated to bf16, q = L - r rounded to the
+ *     storage, magnitudes times damping, L = store(q + store(r)));  LDPC_CIRC_SCALAR: the stepper's
+ *     scalar path (exact constants, q unrounded, L = store(q + r)), damping must be 1;
+ *   - stop LDPC_CIRC_STOP_SYNDROME: the stepper (full syndrome after every iteration; a frame that
+ *     never meets it is a frame error, with bit errors = info positions holding a value <= 0);
+ *     LDPC_CIRC_STOP_GENIE: the engine on silicon (stop once no info position has its sign bit set;
+ *     bit errors = info sign bits of a frame that never stopped, reader_brisc.cpp:166-198,
+ *     writer_ncrisc.cpp:265-337).  Info positions are the first N - M columns.
+ * Tallies and per-frame outputs of LDPC_ALGO_CIRC runs follow that engine (ldpc_tally.bit_errors
+ * then counts info positions).  The defaults (before any call) are the silicon engine: SFPU,
+ * damping 0.9375, genie stop.  LDPC_ENOTSUP for codes whose rows are not of degrees 3 and 6. */
+#define LDPC_CIRC_SCALAR 0
+#define LDPC_CIRC_SFPU 1
+#define LDPC_CIRC_STOP_SYNDROME 0
+#define LDPC_CIRC_STOP_GENIE 1
+typedef struct {
+    int32_t numerics;  /* LDPC_CIRC_SFPU or LDPC_CIRC_SCALAR */
+    int32_t stop;      /* LDPC_CIRC_STOP_SYNDROME or LDPC_CIRC_STOP_GENIE */
+    float damping;     /* in (0, 1]; the engine's beta = 15/16 */
+    int32_t reserved0; /* 0 */
+} ldpc_circ_config;
+int ldpc_set_circulant(ldpc_handle* h, const ldpc_circ_config* c);
 
 /* ---- Weighted Approximate-Min* decoder (training path; no counterpart in the reference) ----
  * Layered decoding of the handle's QC code for exactly n_iter iterations (no early stop) with

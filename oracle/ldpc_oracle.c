@@ -259,8 +259,9 @@ int oracle_decode_nostop(int N, int M, int P, int dmax, const int32_t* rows, con
  *                       meets it is a frame error with bit errors = info positions with value <= 0;
  *   CIRC_STOP_GENIE     the device engine (engines/circulant_dma_4cw/reader_brisc.cpp:166-198,
  *                       writer_ncrisc.cpp:265-337): stop once no info position has its sign bit
- *                       set; a frame that never stops is a frame error with bit errors = info
- *                       positions with the sign bit set.
+ *                       set; a frame that never stops has bit errors = info positions with the sign
+ *                       bit set, and is a frame error when that count is non-zero (always, unless
+ *                       max_iter = 0).
  * A frame that stops reports zero bit errors, as both do.
  */
 #define CIRC_SCALAR 0
@@ -378,7 +379,9 @@ int oracle_circ_decode(int N, int M, int P, int dmax, const int32_t* rows, const
         for (int i = 0; i < n_info; i++)
             be += stop == CIRC_STOP_GENIE ? (int)(f2u(L[i]) >> 31) : (L[i] <= 0.0f);
     *bit_errors = be;
-    *frame_error = !stopped;
+    /* the device engine counts a frame error when an unstopped frame has an info error
+     * (writer_ncrisc.cpp:333); the stepper when the frame never met the syndrome (:804-806) */
+    *frame_error = stop == CIRC_STOP_GENIE ? be > 0 : !stopped;
     return 0;
 }
 

@@ -35,6 +35,7 @@ def test_struct_layouts():
     assert C.sizeof(capi.RunParams) == 72
     assert C.sizeof(capi.Tally) == 64
     assert C.sizeof(capi.WdecConfig) == 6 * 4 + 12 * 18 * 4
+    assert C.sizeof(capi.CircConfig) == 16
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
@@ -58,3 +59,4 @@ def test_bad_arguments_are_rejected_before_any_device_work():
     assert lib.ldpc_create(C.byref(m), 0, C.byref(h)) == -22
     t = capi.Tally()
     assert lib.ldpc_run_chunk(None, None, C.byref(t)) == -22
+    assert lib.ldpc_set_circulant(None, C.byref(capi.CircConfig(1, 1, 0.9375, 0))) == -22

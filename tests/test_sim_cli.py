@@ -110,6 +110,34 @@ def test_circulant_style_csv(matrix_file, tmp_path):
     assert list(df.Total_Blocks) == [1000, 2000] and df.Mean_Iterations.iloc[-1] == 5.0
 
 
+class CircStubEngine(StubEngine):
+    """The stub with the circulant hook: records the settings ldpc_sim passes."""
+    settings = []
+
+    def set_circulant(self, o):
+        CircStubEngine.settings.append((o.circulant, o.damping))
+
+
+def test_circulant_modes(matrix_file):
+    o = sim.parse_args(["--circulant", "device"])
+    assert o.circulant == "device" and o.damping is None
+    assert sim.CIRC_MODES["device"] == (1, 1, 0.9375) and sim.CIRC_MODES["stepper"] == (0, 0, 1.0)
+    for bad in (["--circulant", "tile"], ["--damping", "0.9"], ["--circulant", "device", "-n"],
+                ["--circulant", "stepper", "-R", "3"]):
+        out = io.StringIO()
+        assert sim.main(["-c", matrix_file] + bad, engine_factory=CircStubEngine, out=out) == 2
+    out = io.StringIO()
+    CircStubEngine.settings = []
+    rc = sim.main(["-c", matrix_file, "-p", "512", "-t", "999", "-k", "1000", "-b", "1000", "-s",
+                   "--circulant", "stepper-sfpi", "--damping", "0.9"], engine_factory=CircStubEngine, out=out)
+    assert rc == 0 and CircStubEngine.settings == [("stepper-sfpi", 0.9)]
+    lines = out.getvalue().splitlines()
+    assert any("circulant engine (stepper-sfpi: SFPU arithmetic" in l and "damping 0.9" in l for l in lines)
+    prog = json_lines(lines)[0]
+    # BER over the K = 1024 info positions, as the circulant engine reports it
+    assert prog["ber"] == pytest.approx(prog["bit_errors"] / (prog["blocks"] * 1024), rel=1e-5)
+
+
 def _reference_script(name):
     p = os.path.join(REFERENCE, name)
     if not os.path.exists(p):

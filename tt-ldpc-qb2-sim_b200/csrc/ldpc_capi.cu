@@ -93,6 +93,8 @@ struct ldpc_handle {
     // weights of LDPC_ALGO_WAMIN runs
     float2* d_wtab = nullptr;  // [w_iters][w_slots] (alpha, beta) per iteration and edge slot
     int w_iters = 0, w_slots = 0;
+    // settings of LDPC_ALGO_CIRC runs (default: the circulant engine on silicon)
+    ldpc_circ_config circ{LDPC_CIRC_SFPU, LDPC_CIRC_STOP_GENIE, 0.9375f, 0};
     unsigned long long* h_tally = nullptr;  // pinned
     int64_t launches = 0;
 };
@@ -315,6 +317,21 @@ extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float*
     return 0;
 }
 
+extern "C" int ldpc_set_circulant(ldpc_handle* h, const ldpc_circ_config* c) {
+    if (!h) return fail(LDPC_EINVAL, "handle is NULL");
+    if (!c) return fail(LDPC_EINVAL, "config is NULL");
+    if (c->numerics != LDPC_CIRC_SCALAR && c->numerics != LDPC_CIRC_SFPU)
+        return fail(LDPC_EINVAL, "unknown circulant numerics %d", c->numerics);
+    if (c->stop != LDPC_CIRC_STOP_SYNDROME && c->stop != LDPC_CIRC_STOP_GENIE)
+        return fail(LDPC_EINVAL, "unknown circulant stop rule %d", c->stop);
+    if (!(c->damping > 0.0f && c->damping <= 1.0f)) return fail(LDPC_EINVAL, "damping must lie in (0, 1]");
+    if (c->numerics == LDPC_CIRC_SCALAR && c->damping != 1.0f)
+        return fail(LDPC_EINVAL, "the scalar stepper has no damping (damping must be 1)");
+    if (c->reserved0 != 0) return fail(LDPC_EINVAL, "reserved0 must be 0");
+    h->circ = *c;
+    return 0;
+}
+
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
@@ -324,7 +341,8 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
     bool any = reset;
     auto built = [&](int s) {
-        return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G);
+        return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G) ||
+               find_shape(h, s, LDPC_ALGO_CIRC, 0, 0, R, F, B, G);
     };
     for (int s = lo; s <= hi; ++s) any |= built(s);
     if (!any)
@@ -340,7 +358,7 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
 }
 
 extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo, int32_t* shapes, int max_shapes) {
-    if (!h || storage < 0 || storage > 2 || algo < 0 || algo > 2 || (max_shapes > 0 && !shapes))
+    if (!h || storage < 0 || storage > 2 || algo < 0 || algo > 3 || (max_shapes > 0 && !shapes))
         return fail(LDPC_EINVAL, "bad arguments");
     if (h->kind != LDPC_KERNEL_QC) return 0;
     int n = 0;
@@ -368,7 +386,13 @@ static int check_params(const ldpc_handle* h, const ldpc_run_params* p) {
     if (!p) return fail(LDPC_EINVAL, "params are NULL");
     if (p->max_iter < 0 || p->max_iter > 1000000) return fail(LDPC_EINVAL, "max_iter %d out of range", p->max_iter);
     if (p->storage < 0 || p->storage > 2) return fail(LDPC_EINVAL, "unknown storage mode %d", p->storage);
-    if (p->algo < 0 || p->algo > 2) return fail(LDPC_EINVAL, "unknown algorithm %d", p->algo);
+    if (p->algo < 0 || p->algo > 3) return fail(LDPC_EINVAL, "unknown algorithm %d", p->algo);
+    if (p->algo == LDPC_ALGO_CIRC) {
+        if (h->kind != LDPC_KERNEL_QC || h->D != 6)
+            return fail(LDPC_ENOTSUP, "the circulant engine's decoder needs a QC code with rows of degrees 3 and 6");
+        if (p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f)
+            return fail(LDPC_ENOTSUP, "the circulant engine's decoder takes no clips");
+    }
     if (p->algo == LDPC_ALGO_WAMIN) {
         if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
         if (h->w_iters <= 0) return fail(LDPC_EINVAL, "weighted decoding without weights (ldpc_set_weights)");
@@ -446,6 +470,35 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
         qp.wtab = h->d_wtab;
         qp.w_iters = h->w_iters;
         qp.w_slots = h->w_slots;
+    }
+    if (p->algo == LDPC_ALGO_CIRC) {
+        // the engine's edge order is ascending column: inside a layer every edge has its own column
+        // block, so sort the layer's edges by block (the messages follow the same order)
+        for (int l = 0; l < QC_LAYERS; ++l) {
+            const int d = l < 4 ? QC_DEG_LOW : h->D;
+            for (int a = 1; a < d; ++a)
+                for (int b = a; b > 0 && qp.blk_off[l][b - 1] > qp.blk_off[l][b]; --b) {
+                    std::swap(qp.blk_off[l][b - 1], qp.blk_off[l][b]);
+                    std::swap(qp.shift[l][b - 1], qp.shift[l][b]);
+                }
+        }
+        const bool sfpu = h->circ.numerics == LDPC_CIRC_SFPU;
+        // the SFPU kernel's constants are bf16 (sFloat16b truncates the fp32 value)
+        auto c = [&](float v) {
+            uint32_t u;
+            memcpy(&u, &v, 4);
+            if (sfpu) u &= 0xFFFF0000u;
+            memcpy(&v, &u, 4);
+            return v;
+        };
+        qp.circ_c[0] = c(0.69315f);
+        qp.circ_c[1] = c(-0.40f);
+        qp.circ_c[2] = c(0.65715f);
+        qp.circ_c[3] = c(-0.328f);
+        qp.circ_damping = h->circ.damping;
+        qp.circ_sfpu = sfpu ? 1 : 0;
+        qp.stop_rule = h->circ.stop == LDPC_CIRC_STOP_GENIE ? QC_STOP_GENIE : QC_STOP_SYNDROME;
+        qp.n_info = h->N - h->M;
     }
     const int T = h->Z / R;
     int32_t off = 0;
@@ -542,6 +595,9 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
         if (h->kind == LDPC_KERNEL_QC) rc = launch_qc(h, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be);
         if (rc == LDPC_ENOTSUP && p->algo == LDPC_ALGO_WAMIN)
             return fail(LDPC_ENOTSUP, "the weighted decoder is not built for Z=%d D=%d with storage %d", h->Z, h->D,
+                        p->storage);
+        if (rc == LDPC_ENOTSUP && p->algo == LDPC_ALGO_CIRC)
+            return fail(LDPC_ENOTSUP, "the circulant engine's decoder is not built for Z=%d with storage %d", h->Z,
                         p->storage);
         if (rc == LDPC_ENOTSUP) {  // no QC variant for these options: the general kernel decodes any matrix
             if (!h->gen_built) {

@@ -18,7 +18,7 @@
 namespace ldpcb200 {
 
 enum Storage : int { STORE_BF16 = 0, STORE_FP32 = 1, STORE_FP16 = 2 };
-enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2 };
+enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2, ALGO_CIRC = 3 };
 
 // ------------------------------------------------------------------ Philox-4x32-10
 struct U32x4 { uint32_t x, y, z, w; };
@@ -101,6 +101,19 @@ __device__ __forceinline__ float amin_step_fma(float m, float a) {
     const float t = __fmaf_rn(-c1, f05, cur);
     const float u = __fmaf_rn(-c2, __fsub_rn(f2, f05), t);
     return fmaxf(u, 0.0f);
+}
+
+// The circulant engine's min* (tests/test_circulant_dma_stepper.cpp:39-54 and
+// engines/tile_matrix_4cw/sfpi_host_emu.h:590-607): max(min(a, b) - max(c1 + k1 d, c2 + k2 d, 0), 0)
+// with d = |a - b|, every product and sum rounded on its own (no fused multiply-add), so it equals the
+// reference's fp32 expression bit for bit.  a, b >= +0; the result is never -0.
+struct CircConsts { float c1, k1, c2, k2; };
+__device__ __forceinline__ float circ_g(float a, float b, const CircConsts& k) {
+    const float mn = fminf(a, b), mx = fmaxf(a, b);
+    const float d = __fsub_rn(mx, mn);
+    const float l1 = __fadd_rn(k.c1, __fmul_rn(k.k1, d));
+    const float l2 = __fadd_rn(k.c2, __fmul_rn(k.k2, d));
+    return fmaxf(__fsub_rn(mn, fmaxf(fmaxf(l1, l2), 0.0f)), 0.0f);
 }
 
 }  // namespace ldpcb200

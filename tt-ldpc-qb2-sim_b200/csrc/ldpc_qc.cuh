@@ -64,7 +64,20 @@ struct QcParams {
     // qc_edge_slot(l, e, D); iteration t uses row min(t, w_iters - 1)
     const float2* wtab;
     int32_t w_iters, w_slots;
+    // ALGO_CIRC stop rule and tally (the circulant engine's): QC_STOP_SYNDROME tests the syndrome
+    // after every iteration; QC_STOP_GENIE stops a frame once none of its info positions
+    // 0..n_info-1 has the sign bit set (the engine on silicon).  Other algorithms follow the
+    // reference engine: syndrome from the third iteration on, bit errors over the first N-P positions.
+    int32_t stop_rule;
+    int32_t n_info;
+    // ALGO_CIRC: the min* constants (c1, k1, c2, k2), the damping factor, and the arithmetic form
+    // (circ_sfpu = 1: q and r rounded to storage before use, as the SFPU kernels do)
+    float circ_c[4];
+    float circ_damping;
+    int32_t circ_sfpu;
 };
+
+enum QcStop : int { QC_STOP_SYNDROME = 0, QC_STOP_GENIE = 1 };
 
 // Slot of edge e of layer l in a per-iteration row of the weight table: layers 0-3 (degree 3) first.
 __host__ __device__ constexpr int qc_edge_slot(int l, int e, int D) {
@@ -256,6 +269,76 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
             float ln = __fadd_rn(q[f][e], rn[e]);
             if (CLIP) ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
             LT::st(lptr(f, e), 0, ln);
+        }
+#pragma unroll
+        for (int e = 0; e < d; e += 2) rm[f].set2(e, rn[e], (e + 1 < d) ? rn[e + 1] : 0.0f);
+    }
+}
+
+// Storage rounding of a check message (what RowMsg::set2 / RTraits::st keep).
+template <int MODE> __device__ __forceinline__ float msg_round(float v) {
+    if constexpr (MODE == STORE_BF16) return bf16_round(v);
+    else if constexpr (MODE == STORE_FP16) return fp16_round_sat(v);
+    else return v;
+}
+
+// ALGO_CIRC: one row of the circulant engine's decoder (degree 3 or 6; edges in ascending column
+// order).  The degree-6 magnitudes come from the pairwise min* tree of
+// tests/test_circulant_dma_stepper.cpp:404-425 and engines/circulant_dma_4cw/compute_trisc.cpp:
+// 370-460: m03 = g(a0, a3), m14 = g(a1, a4), m25 = g(a2, a5); edge 0 gets g(g(m14, m25), a3), edge 3
+// g(g(m14, m25), a0), and likewise for the pairs (1, 4) and (2, 5); a degree-3 row gives each edge g
+// of the other two (:436-446).  Each magnitude is scaled by the damping factor, signed with the
+// parity of the other edges, and r and L are stored with the storage rounding.  SFPU form
+// (cs.sfpu): q is rounded to storage first and L = store(q + store(r)) (compute_trisc.cpp:351-360,
+// 387-395); scalar form: L = store(q + r) with r unrounded (test_circulant_dma_stepper.cpp:452-456).
+struct CircRt {
+    CircConsts k;
+    float damping;
+    bool sfpu;
+};
+template <int d, int MODE, int F, class MSG, bool BO = false>
+__device__ __forceinline__ void row_update_circ(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
+                                                MSG (&rm)[F], const CircRt& cr) {
+    static_assert(d == 3 || d == 6, "the circulant engine's rows have degree 3 or 6");
+    using LT = LTraits<MODE>;
+    using LE = typename LT::T;
+    auto lptr = [&](int f, int e) -> LE* {
+        if constexpr (BO) return reinterpret_cast<LE*>(reinterpret_cast<char*>(sL + f * lstride) + idx[e]);
+        else return sL + f * lstride + idx[e];
+    };
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+        float q[d], a[d], mag[d];
+        uint32_t par = 0;
+#pragma unroll
+        for (int e = 0; e < d; ++e) {
+            q[e] = __fsub_rn(LT::ld(lptr(f, e), 0), rm[f].get(e));
+            if (cr.sfpu) q[e] = LT::round_ch(q[e]);
+            par ^= __float_as_uint(q[e]);
+            a[e] = fabsf(q[e]);
+        }
+        par &= 0x80000000u;
+        if constexpr (d == 6) {
+            const float m03 = circ_g(a[0], a[3], cr.k), m14 = circ_g(a[1], a[4], cr.k), m25 = circ_g(a[2], a[5], cr.k);
+            const float o0 = circ_g(m14, m25, cr.k), o1 = circ_g(m03, m25, cr.k), o2 = circ_g(m03, m14, cr.k);
+            mag[0] = circ_g(o0, a[3], cr.k);
+            mag[3] = circ_g(o0, a[0], cr.k);
+            mag[1] = circ_g(o1, a[4], cr.k);
+            mag[4] = circ_g(o1, a[1], cr.k);
+            mag[2] = circ_g(o2, a[5], cr.k);
+            mag[5] = circ_g(o2, a[2], cr.k);
+        } else {
+            mag[0] = circ_g(a[1], a[2], cr.k);
+            mag[1] = circ_g(a[0], a[2], cr.k);
+            mag[2] = circ_g(a[0], a[1], cr.k);
+        }
+        float rn[d];
+#pragma unroll
+        for (int e = 0; e < d; ++e) {
+            rn[e] = __uint_as_float(__float_as_uint(__fmul_rn(mag[e], cr.damping)) |
+                                    (par ^ (__float_as_uint(q[e]) & 0x80000000u)));
+            const float rs = msg_round<MODE>(rn[e]);
+            LT::st(lptr(f, e), 0, __fadd_rn(q[e], cr.sfpu ? rs : rn[e]));
         }
 #pragma unroll
         for (int e = 0; e < d; e += 2) rm[f].set2(e, rn[e], (e + 1 < d) ? rn[e + 1] : 0.0f);
@@ -469,6 +552,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                   "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
     using RE = typename RTraits<MODE>::T;
     static_assert(!OT || (!PAIR && !RG && R == 1), "the offset table is built for one row per thread");
+    constexpr bool CIRC = ALGO == ALGO_CIRC;
+    static_assert(!CIRC || (D == 6 && !CLIP && !PAIR), "the circulant engine's decoder: degrees 3 and 6, no clips");
     using SV = SlotView<MODE, PAIR>;
     using LT = LTraits<MODE>;
     using LE = typename LT::T;
@@ -487,11 +572,13 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     __shared__ uint32_t s_fid[QC_MAX_F];
     __shared__ uint32_t s_sfail[QC_MAX_F];
     __shared__ uint32_t s_be[QC_MAX_F];
+    __shared__ uint32_t s_iz[QC_MAX_F];  // ALGO_CIRC: info positions with value <= 0
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
+    const CircRt cr{CircConsts{p.circ_c[0], p.circ_c[1], p.circ_c[2], p.circ_c[3]}, p.circ_damping, p.circ_sfpu != 0};
 
     MsgRegs<D, R, F, MODE, PAIR, RG> msg;
     if constexpr (OT) {  // each thread writes and later reads only its own entries: no barrier needed
@@ -596,65 +683,84 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             for (int f = 0; f < F; ++f)
                 wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_slots : nullptr;
             // OT: each layer's offsets are loaded one layer ahead, so their shared-memory latency
-            // overlaps the previous row update
+            // overlaps the previous row update.  ALGO_CIRC visits the degree-D layers first (the
+            // circulant engine's tile schedule, rows 512..1535 before 0..511 for K = 1024:
+            // engines/circulant_dma_4cw/ar4ja_circulant_descriptors_4cw.h:29-31).
             int pre[OT ? D : 1];
-            if constexpr (OT) ot_load<QC_DEG_LOW, T>(sOT, tid, pre);
+            if constexpr (OT) {
+                if constexpr (CIRC) ot_load<D, T>(sOT + T * ot_layer_start(4, D), tid, pre);
+                else ot_load<QC_DEG_LOW, T>(sOT, tid, pre);
+            }
 #pragma unroll
             for (int l = 0; l < QC_LAYERS; ++l) {
+                const int ly = CIRC ? (l + 4) % QC_LAYERS : l;        // the layer updated at step l
+                const int ly_next = CIRC ? (l + 5) % QC_LAYERS : l + 1;
                 const float2* wl[F];
 #pragma unroll
-                for (int f = 0; f < F; ++f) wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(l, 0, D) : nullptr;
+                for (int f = 0; f < F; ++f) wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(ly, 0, D) : nullptr;
+                int cur[OT ? D : 1];
+                if constexpr (OT) {  // this layer's offsets; start loading the next layer's
+#pragma unroll
+                    for (int e = 0; e < D; ++e) cur[e] = pre[e];
+                    if (l + 1 < QC_LAYERS) {
+                        if (ly_next < 4) ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(ly_next, D), tid, pre);
+                        else ot_load<D, T>(sOT + T * ot_layer_start(ly_next, D), tid, pre);
+                    }
+                }
 #pragma unroll
                 for (int rho = 0; rho < R; ++rho) {
                     const int j = tid + rho * T;
-                    if (l < 4) {
+                    if (ly < 4) {
                         int idx[QC_DEG_LOW];
                         if constexpr (OT) {
 #pragma unroll
-                            for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = pre[e];
-                            if (l + 1 < 4)
-                                ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
-                            else
-                                ot_load<D, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
+                            for (int e = 0; e < QC_DEG_LOW; ++e) idx[e] = cur[e];
                         } else
 #pragma unroll
                             for (int e = 0; e < QC_DEG_LOW; ++e)
-                                idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                                idx[e] = p.blk_off[ly][e] + ((j + p.shift[ly][e]) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<QC_DEG_LOW, MODE> rm[F];
 #pragma unroll
                             for (int f = 0; f < F; ++f)
                                 rm[f] = RowMsgGlobal<QC_DEG_LOW, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
-                                        p.layer_off[l] + j, Z};
-                            row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
+                                        p.layer_off[ly] + j, Z};
+                            if constexpr (CIRC) row_update_circ<QC_DEG_LOW, MODE, F>(idx, sL, lstride, rm, cr);
+                            else row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
-                            row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[l & 3]);
+                            row_update_pair<QC_DEG_LOW, MODE>(idx, sL, msg.r3[ly & 3]);
+                        else if constexpr (CIRC)
+                            row_update_circ<QC_DEG_LOW, MODE, F, RowMsg<QC_DEG_LOW, MODE>, OT>(
+                                idx, sL, lstride, msg.r3[ly & 3][rho], cr);
                         else
                             row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F, RowMsg<QC_DEG_LOW, MODE>, OT>(
-                                idx, sL, lstride, msg.r3[l & 3][rho], r_cap, lp_cap, wl);
+                                idx, sL, lstride, msg.r3[ly & 3][rho], r_cap, lp_cap, wl);
                     } else {
                         int idx[D];
                         if constexpr (OT) {
 #pragma unroll
-                            for (int e = 0; e < D; ++e) idx[e] = pre[e];
-                            if (l + 1 < QC_LAYERS) ot_load<D, T>(sOT + T * ot_layer_start(l + 1, D), tid, pre);
+                            for (int e = 0; e < D; ++e) idx[e] = cur[e];
                         } else
 #pragma unroll
-                            for (int e = 0; e < D; ++e) idx[e] = p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1));
+                            for (int e = 0; e < D; ++e) idx[e] = p.blk_off[ly][e] + ((j + p.shift[ly][e]) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<D, MODE> rm[F];
 #pragma unroll
                             for (int f = 0; f < F; ++f)
                                 rm[f] = RowMsgGlobal<D, MODE>{
                                     reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
-                                        p.layer_off[l] + j, Z};
-                            row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
+                                        p.layer_off[ly] + j, Z};
+                            if constexpr (CIRC) row_update_circ<D, MODE, F>(idx, sL, lstride, rm, cr);
+                            else row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
-                            row_update_pair<D, MODE>(idx, sL, msg.rD[(l - 4) & 7]);
+                            row_update_pair<D, MODE>(idx, sL, msg.rD[(ly - 4) & 7]);
+                        else if constexpr (CIRC)
+                            row_update_circ<D, MODE, F, RowMsg<D, MODE>, OT>(idx, sL, lstride,
+                                                                            msg.rD[(ly - 4) & 7][rho], cr);
                         else
                             row_update<D, MODE, ALGO, CLIP, F, RowMsg<D, MODE>, OT>(
-                                idx, sL, lstride, msg.rD[(l - 4) & 7][rho], r_cap, lp_cap, wl);
+                                idx, sL, lstride, msg.rD[(ly - 4) & 7][rho], r_cap, lp_cap, wl);
                     }
                 }
                 __syncthreads();
@@ -668,7 +774,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
 #pragma unroll
         for (int f = 0; f < F; ++f)
             if ((act >> f) & 1u)
-                if (it[f] >= 3 || it[f] >= p.max_iter) eval |= 1u << f;
+                if (it[f] >= (CIRC ? 1 : 3) || it[f] >= p.max_iter) eval |= 1u << f;
         if (!eval) continue;
 
         const int nwords = nblk * W;
@@ -682,7 +788,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 if (lane == 0) hb[wd] = b;
             }
         }
-        if (tid < F) { s_sfail[tid] = 0; s_be[tid] = 0; }
+        if (tid < F) { s_sfail[tid] = 0; s_be[tid] = 0; s_iz[tid] = 0; }
         __syncthreads();
         // syndrome words: (f, layer, word) -> XOR over the layer's edges of the rotated block vectors
         for (int t = tid; t < F * QC_LAYERS * W; t += T) {
@@ -702,8 +808,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             }
             if (acc) atomicAdd(&s_sfail[f], (uint32_t)__popc(acc));
         }
-        // bit errors over the transmitted prefix
-        const int ntxw = p.n_tx >> 5;
+        // bit errors over the transmitted prefix (ALGO_CIRC: sign bits over the info positions)
+        const int ntxw = CIRC ? p.n_info >> 5 : p.n_tx >> 5;
 #pragma unroll
         for (int f = 0; f < F; ++f) {
             if (!((eval >> f) & 1u)) continue;
@@ -714,30 +820,64 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             if (lane == 0 && cnt) atomicAdd(&s_be[f], cnt);
         }
         __syncthreads();
-        uint32_t done = 0;
+        uint32_t done = 0, stopped = 0;
 #pragma unroll
         for (int f = 0; f < F; ++f) {
             if (!((eval >> f) & 1u)) continue;
-            const bool conv = it[f] >= 3 && s_sfail[f] == 0;
+            bool conv;
+            if constexpr (CIRC)
+                conv = it[f] >= 1 && (p.stop_rule == QC_STOP_GENIE ? s_be[f] == 0 : s_sfail[f] == 0);
+            else
+                conv = it[f] >= 3 && s_sfail[f] == 0;
+            if (conv) stopped |= 1u << f;
             if (conv || it[f] >= p.max_iter) done |= 1u << f;
         }
         if (!done) continue;
+        if constexpr (CIRC) {
+            // the circulant stepper's tally of a frame that never met the syndrome: info positions
+            // with value <= 0 (tests/test_circulant_dma_stepper.cpp:807-816)
+            const uint32_t zc = p.stop_rule == QC_STOP_GENIE ? 0u : (done & ~stopped);
+            if (zc) {
+#pragma unroll
+                for (int f = 0; f < F; ++f) {
+                    if (!((zc >> f) & 1u)) continue;
+                    const SV L(sL, f, lstride);
+                    uint32_t cnt = 0;
+                    for (int i = tid; i < p.n_info; i += T) cnt += L.ld(i) <= 0.0f;
+                    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+                    if (lane == 0 && cnt) atomicAdd(&s_iz[f], cnt);
+                }
+                __syncthreads();
+            }
+        }
 #pragma unroll
         for (int f = 0; f < F; ++f) {
             if (!((done >> f) & 1u)) continue;
-            const uint32_t be = s_be[f], sf = s_sfail[f];
+            uint32_t be = s_be[f];
+            const uint32_t sf = s_sfail[f];
+            bool fe = be > 0;
+            if constexpr (CIRC) {  // a frame that stopped counts no errors; the stepper's frame error
+                const bool st = (stopped >> f) & 1u;  // is "never met the syndrome"
+                if (p.stop_rule == QC_STOP_GENIE) {
+                    be = st ? 0u : be;
+                    fe = be > 0;
+                } else {
+                    be = st ? 0u : s_iz[f];
+                    fe = !st;
+                }
+            }
             if (tid == 0) {
                 t_frames += 1;
                 t_be += be;
                 t_be2 += (unsigned long long)be * be;
-                t_fe += be > 0;
+                t_fe += fe;
                 t_it += (unsigned)it[f];
                 t_unc += sf != 0;
                 t_max = max(t_max, (unsigned long long)it[f]);
                 if (p.hist) atomicAdd(&p.hist[min(it[f], p.hist_bins - 1)], 1ull);
                 if (per_frame_snr && p.snr_bins) {
                     atomicAdd(&p.snr_bins[snr_bin[f]], 1ull);
-                    atomicAdd(&p.snr_bins[SNR_BINS + snr_bin[f]], (unsigned long long)(be > 0));
+                    atomicAdd(&p.snr_bins[SNR_BINS + snr_bin[f]], (unsigned long long)fe);
                     atomicAdd(&p.snr_bins[2 * SNR_BINS + snr_bin[f]], (unsigned long long)be);
                     atomicAdd(&p.snr_bins[3 * SNR_BINS + snr_bin[f]], (unsigned long long)it[f]);
                 }

@@ -16,7 +16,9 @@ import numpy as np
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libldpcb200.so")
 
 STORE_BF16, STORE_FP32, STORE_FP16 = 0, 1, 2
-ALGO_AMIN, ALGO_NMS, ALGO_WAMIN = 0, 1, 2
+ALGO_AMIN, ALGO_NMS, ALGO_WAMIN, ALGO_CIRC = 0, 1, 2, 3
+CIRC_SCALAR, CIRC_SFPU = 0, 1
+CIRC_STOP_SYNDROME, CIRC_STOP_GENIE = 0, 1
 KERNEL_QC, KERNEL_GENERAL = 0, 1
 STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 
@@ -24,6 +26,7 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
            "ldpc_channel_llr", "ldpc_channel_llr_device", "ldpc_iter_histogram", "ldpc_snr_bins",
            "ldpc_set_launch_shape", "ldpc_list_shapes", "ldpc_list_shapes_algo", "ldpc_set_weights",
+           "ldpc_set_circulant",
            "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
@@ -59,6 +62,11 @@ class WdecConfig(C.Structure):
     _fields_ = [("n_iter", C.c_int32), ("n_classes", C.c_int32), ("ckpt_every", C.c_int32),
                 ("post_all", C.c_int32), ("fp64", C.c_int32), ("reserved0", C.c_int32),
                 ("edge_class", (C.c_int32 * 18) * 12)]
+
+
+class CircConfig(C.Structure):
+    """ldpc_circ_config: settings of ALGO_CIRC runs (the circulant engine's decoder)."""
+    _fields_ = [("numerics", C.c_int32), ("stop", C.c_int32), ("damping", C.c_float), ("reserved0", C.c_int32)]
 
 
 class Tally(C.Structure):
@@ -101,6 +109,7 @@ def load(path: str = LIB_PATH):
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_list_shapes_algo.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_set_weights.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int, C.c_int, P(C.c_int32)]
+    L.ldpc_set_circulant.argtypes = [C.c_void_p, P(CircConfig)]
     L.ldpc_channel_llr_device.argtypes = [C.c_void_p, P(RunParams), C.c_void_p, C.c_void_p]
     L.ldpc_wdec_workspace_bytes.argtypes = [C.c_void_p, P(WdecConfig), C.c_int64]
     L.ldpc_wdec_workspace_bytes.restype = C.c_int64
@@ -333,6 +342,12 @@ class Decoder:
 
     def clear_weights(self):
         _check(self._lib.ldpc_set_weights(self._h, None, None, 0, 0, None))
+
+    def set_circulant(self, numerics: int = CIRC_SFPU, stop: int = CIRC_STOP_GENIE, damping: float = 0.9375):
+        """Settings of ALGO_CIRC runs: the circulant engine's arithmetic form (CIRC_SFPU: its device
+        kernels; CIRC_SCALAR: its stepper's scalar path, damping 1), stop rule (CIRC_STOP_GENIE: the
+        engine on silicon; CIRC_STOP_SYNDROME: the stepper's Monte Carlo loop) and damping factor."""
+        _check(self._lib.ldpc_set_circulant(self._h, C.byref(CircConfig(numerics, stop, damping, 0))))
 
     def iter_histogram(self, n_bins: int = 256) -> np.ndarray:
         h = np.zeros(n_bins, np.uint64)

@@ -17,8 +17,14 @@ Mirrors ``engines/scalar_5w/ldpc_sim_scalar.cpp`` (lines 271-644):
 Long options add what the GPU engine offers: ``--storage bf16|fp32|fp16`` (default bf16, the
 reference numerics), ``--seed`` (Philox key, default 133742 like the reference's root seed,
 ``:403-407``), ``--device``, ``--out CSV`` (the circulant engine's per-chunk CSV,
-``engines/circulant_dma_4cw/ldpc_sim_circulant_dma.cpp:282-406``) and ``--resume STATE.json``
-(continue a point from its saved frame index and tallies).
+``engines/circulant_dma_4cw/ldpc_sim_circulant_dma.cpp:282-406``), ``--resume STATE.json``
+(continue a point from its saved frame index and tallies) and ``--circulant MODE`` (``--damping X``):
+decode with the circulant engine's arithmetic instead of the scalar engine's, for the rate-1/2
+codes: ``device`` = the engine on silicon (SFPU arithmetic, damping 15/16, stop once no info bit is
+negative, ``engines/circulant_dma_4cw``), ``stepper`` = its golden stepper's scalar path and
+``stepper-sfpi`` its SFPU path (``tests/test_circulant_dma_stepper.cpp --monte-carlo [--sfpi]``:
+syndrome after every iteration, no damping).  Bit errors and BER then count the K info positions,
+as that engine does (``ldpc_sim_circulant_dma.cpp:378``).
 
 Frame f of an Eb/N0 point is decoded from Philox counter (seed, f): every batch takes the next
 ``batch x cores`` frame indices, so a run is reproducible and resumable by its frame index.
@@ -80,13 +86,19 @@ class Options:
     device: int = 0
     out_csv: str = ""
     resume: str = ""
+    circulant: str = ""
+    damping: Optional[float] = None
     extra: dict = field(default_factory=dict)
+
+
+# --circulant modes: (numerics, stop rule, default damping); capi's CIRC_* values
+CIRC_MODES = {"device": (1, 1, 0.9375), "stepper": (0, 0, 1.0), "stepper-sfpi": (1, 0, 1.0)}
 
 
 def parse_args(argv: List[str]) -> Options:
     o = Options()
     opts, _ = getopt.gnu_getopt(argv, "c:e:p:t:m:b:k:i:svnL:R:G:V:",
-                                ["storage=", "seed=", "device=", "out=", "resume="])
+                                ["storage=", "seed=", "device=", "out=", "resume=", "circulant=", "damping="])
     for k, v in opts:
         if k == "-c": o.matrix = v
         elif k == "-e": o.ebn0 = float(v)
@@ -111,6 +123,15 @@ def parse_args(argv: List[str]) -> Options:
         elif k == "--device": o.device = int(v)
         elif k == "--out": o.out_csv = v
         elif k == "--resume": o.resume = v
+        elif k == "--circulant":
+            if v not in CIRC_MODES:
+                raise getopt.GetoptError(f"--circulant must be one of {', '.join(CIRC_MODES)}, not {v}")
+            o.circulant = v
+        elif k == "--damping": o.damping = float(v)
+    if o.damping is not None and not o.circulant:
+        raise getopt.GetoptError("--damping needs --circulant")
+    if o.circulant and (o.nms or o.l_max > 0 or o.r_max > 0 or o.l_post_max > 0 or o.gamma > 0):
+        raise getopt.GetoptError("--circulant takes neither -n nor the -L/-R/-V/-G clips")
     return o
 
 
@@ -134,12 +155,16 @@ class GpuEngine:
     def describe(self) -> str:
         return "layered QC kernel" if self.dec.kind == self.capi.KERNEL_QC else "general file-order kernel"
 
+    def set_circulant(self, o: Options):
+        num, stop, damp = CIRC_MODES[o.circulant]
+        self.dec.set_circulant(num, stop, damp if o.damping is None else o.damping)
+
     def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
         """For long runs of the QC kernel (plain Approximate-Min*, no clips), time every built launch
         shape of the chosen storage on 2^16 frames of this channel (another seed) and keep the
         fastest.  Shapes change only the speed: every shape decodes every frame to the same bits."""
         if (self.dec.kind != self.capi.KERNEL_QC or o.nms or o.r_max > 0 or o.l_post_max > 0 or o.l_max > 0
-                or o.gamma > 0 or max_blocks < TUNE_MIN_BLOCKS):
+                or o.gamma > 0 or o.circulant or max_blocks < TUNE_MIN_BLOCKS):
             return None
         res, _ = self.dec.autotune(mu, sigma, storages=(o.storage,), frames=1 << 16, max_iter=o.max_iter,
                                    repeats=1)
@@ -148,7 +173,8 @@ class GpuEngine:
     def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
         p = self.dec.params(mu=mu, sigma=sigma, seed=o.seed, first_frame=first, n_frames=n,
                             max_iter=o.max_iter, storage=o.storage,
-                            algo=self.capi.ALGO_NMS if o.nms else self.capi.ALGO_AMIN,
+                            algo=(self.capi.ALGO_CIRC if o.circulant else
+                                  self.capi.ALGO_NMS if o.nms else self.capi.ALGO_AMIN),
                             l_max=l_max, r_max=o.r_max, l_post_max=o.l_post_max)
         r = self.dec.run_chunk(p)
         return Batch(r.frames, r.bit_errors, r.frame_errors, r.iter_sum, r.kernel_ms)
@@ -190,6 +216,15 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
     except Exception as e:  # no GPU, library missing, unsupported matrix: fail loudly
         print(f"ldpc_sim: cannot start the GPU engine: {e}", file=sys.stderr)
         return 1
+    if o.circulant:
+        try:
+            engine.set_circulant(o)
+        except Exception as e:  # e.g. a code whose rows are not of degrees 3 and 6
+            print(f"ldpc_sim: the circulant engine's decoder cannot run this matrix: {e}", file=sys.stderr)
+            close = getattr(engine, "close", None)
+            if close:
+                close()
+            return 1
     cores = 1 if o.single_core else MESH_CORES
     say(f"[CONFIG] Running in {'SINGLE-CORE' if o.single_core else 'MULTI-CORE'} accounting "
         f"({cores} cores) on one GPU with the {engine.describe()}")
@@ -201,9 +236,16 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
         batch = o.blocks_per_core
     say(f"[CONFIG] Stopping criteria: min {o.target_fe} block errors OR max {o.blocks_per_core} blocks/core "
         f"(Batch size/core: {batch}, max mesh blocks: {max_blocks}, max iters: {o.max_iter})")
-    say("[CONFIG] Decoder algorithm: " + ("Normalized Min-Sum (alpha=0.75)" if o.nms else
-                                           "Approximate-Min* (Christopher Jones MILCOM 2003)")
-        + f", message storage {o.storage}")
+    if o.circulant:
+        num, stop, damp = CIRC_MODES[o.circulant]
+        damp = damp if o.damping is None else o.damping
+        say(f"[CONFIG] Decoder algorithm: circulant engine ({o.circulant}: "
+            f"{'SFPU' if num else 'scalar'} arithmetic, pairwise Approximate-Min* tree, damping {_g(damp)}, "
+            f"{'info-bit' if stop else 'syndrome'} stop), message storage {o.storage}")
+    else:
+        say("[CONFIG] Decoder algorithm: " + ("Normalized Min-Sum (alpha=0.75)" if o.nms else
+                                               "Approximate-Min* (Christopher Jones MILCOM 2003)")
+            + f", message storage {o.storage}")
     rate = (mat.N - mat.M) / (mat.N - o.punctured)
     snr = 10.0 ** (o.ebn0 / 10.0)
     mu = float(np.float32(4.0 * rate * snr))
@@ -243,6 +285,7 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
         say(f" [CSV] Logging to: {o.out_csv}")
 
     ntx = mat.N - o.punctured
+    ber_bits = (mat.N - mat.M) if o.circulant else ntx  # the circulant engine's BER is over info bits
     t0 = time.perf_counter()
     try:
         while fe < o.target_fe and blocks < max_blocks:
@@ -275,7 +318,7 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
             iters += r.iter_sum
             kernel_ms += r.kernel_ms
             el = time.perf_counter() - t0
-            ber = be / (blocks * ntx) if blocks else 0.0
+            ber = be / (blocks * ber_bits) if blocks else 0.0
             fer = fe / blocks if blocks else 0.0
             msps = (blocks * ntx / el) / 1e6 if el > 0 else 0.0
             say("{" + f"\"progress\": true, \"ebn0\": {_g(o.ebn0)}, \"blocks\": {blocks}, "
