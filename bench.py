@@ -211,6 +211,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "circulant":
+        return run_reference_circulant(args)
     from oracle import oracle as O
     code = code_and_matrix()
     oc = O.Code(code.row_matrix(), code.N, code.P)
@@ -636,6 +638,47 @@ def circ_cpu_baseline(seconds: float, threads: int):
                        f"FER {fe / max(blocks, 1):.2e}")}
 
 
+def run_reference_circulant(args):
+    """Reference arm of the circulant workload: the reference's golden stepper Monte Carlo (scalar
+    path) on every host thread, K steps of about --ref-step-seconds per Eb/N0 point."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    if O.ref_binary("ref_circ_mc") is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_circ_mc is not built "
+                          "(make -C oracle ref with the reference tree present)"}), flush=True)
+        return 0
+    sizes = {}
+    for eb in POINTS:
+        b0, _, _, t0 = ref_circ_mc(eb, 4 * threads * 64, threads)
+        sizes[eb] = max(4 * threads, int(b0 * args.ref_step_seconds / max(t0, 1e-3)))
+    frames = fe = 0
+    el = 0.0
+    for step in range(args.warmup + args.steps):
+        for eb in POINTS:
+            b, e, _, t = ref_circ_mc(eb, sizes[eb], threads)
+            if step >= args.warmup:
+                frames += b; fe += e; el += t
+    value = frames * 2048 / el / 1e9 if el > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * el / max(args.steps, 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: all-zero codeword, BPSK over AWGN, the stepper's std::normal_distribution channel",
+        "impl": "reference",
+        "config": {"workload": "circulant engine's decoder on AR4JA r1/2 K=1024 N=2560, Eb/N0 2.5 and 3.0 dB, "
+                               "max 200 iterations",
+                   "engine": "tests/test_circulant_dma_stepper.cpp --monte-carlo (scalar path, syndrome stop) "
+                             "on host threads",
+                   "frames_per_s": round(frames / el, 1) if el > 0 else 0.0, "fer": fe / max(frames, 1)},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{frames} frames over {el:.1f} s in {args.steps} steps of about "
+                                   f"{args.ref_step_seconds:.1f} s per Eb/N0 point"},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_circulant(args):
     """The circulant engine's decoder on the error-floor points (one GPU, or replicas)."""
     import torch
@@ -672,6 +715,9 @@ def run_circulant(args):
             flush.zero_()
         return out
 
+    dec.set_circulant(*CIRC_SETTINGS["device"])
+    mu, sigma = mus[POINTS[0]]
+    tuned, _ = dec.autotune(mu, sigma, storages=("bf16",), frames=1 << 18, max_iter=MAX_ITER, algo=capi.ALGO_CIRC)
     res = {}
     for mode in ("stepper", "device"):  # the headline mode last
         nsteps = args.steps if mode == "device" else max(1, args.steps // 4)
@@ -725,6 +771,9 @@ def run_circulant(args):
             "points": {str(eb): {"frames": a[0], "frame_errors": a[1], "bit_errors": a[2],
                                  "mean_iters": round(a[3] / max(a[0], 1), 4),
                                  "gsps": round(a[0] * code.n_tx / (a[4] / 1e3) / 1e9, 3)} for eb, a in acc.items()},
+            "autotune": {st: {"shape": list(sh), "mframes_per_s": {",".join(map(str, k)): round(v, 3)
+                                                                     for k, v in tm.items()}}
+                         for st, (sh, tm) in tuned.items()},
             "stepper_mode": {str(eb): {"frames": a[0], "frame_errors": a[1],
                                        "mean_iters": round(a[3] / max(a[0], 1), 4),
                                        "gsps": round(a[0] * code.n_tx / (a[4] / 1e3) / 1e9, 3)}

@@ -160,14 +160,16 @@ class GpuEngine:
         self.dec.set_circulant(num, stop, damp if o.damping is None else o.damping)
 
     def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
-        """For long runs of the QC kernel (plain Approximate-Min*, no clips), time every built launch
-        shape of the chosen storage on 2^16 frames of this channel (another seed) and keep the
-        fastest.  Shapes change only the speed: every shape decodes every frame to the same bits."""
+        """For long runs of the QC kernel (Approximate-Min* or the circulant engine's decoder, no
+        clips), time every built launch shape of the chosen storage on 2^16 frames of this channel
+        (another seed) and keep the fastest.  Shapes change only the speed: every shape decodes every
+        frame to the same bits."""
         if (self.dec.kind != self.capi.KERNEL_QC or o.nms or o.r_max > 0 or o.l_post_max > 0 or o.l_max > 0
-                or o.gamma > 0 or o.circulant or max_blocks < TUNE_MIN_BLOCKS):
+                or o.gamma > 0 or max_blocks < TUNE_MIN_BLOCKS):
             return None
+        algo = self.capi.ALGO_CIRC if o.circulant else self.capi.ALGO_AMIN
         res, _ = self.dec.autotune(mu, sigma, storages=(o.storage,), frames=1 << 16, max_iter=o.max_iter,
-                                   repeats=1)
+                                   repeats=1, algo=algo)
         return res.get(o.storage, (None,))[0]
 
     def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
