@@ -107,13 +107,20 @@ __device__ __forceinline__ float amin_step_fma(float m, float a) {
 // engines/tile_matrix_4cw/sfpi_host_emu.h:590-607): max(min(a, b) - max(c1 + k1 d, c2 + k2 d, 0), 0)
 // with d = |a - b|, every product and sum rounded on its own (no fused multiply-add), so it equals the
 // reference's fp32 expression bit for bit.  a, b >= +0; the result is never -0.
+// |a - b| equals max - min exactly (rounding is symmetric), and the correction max(l1, l2, 0) is one
+// three-input max (sm_100): 9 instructions per min*.
 struct CircConsts { float c1, k1, c2, k2; };
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 __device__ __forceinline__ float circ_g(float a, float b, const CircConsts& k) {
-    const float mn = fminf(a, b), mx = fmaxf(a, b);
-    const float d = __fsub_rn(mx, mn);
+    const float mn = fminf(a, b);
+    const float d = fabsf(__fsub_rn(a, b));
     const float l1 = __fadd_rn(k.c1, __fmul_rn(k.k1, d));
     const float l2 = __fadd_rn(k.c2, __fmul_rn(k.k2, d));
-    return fmaxf(__fsub_rn(mn, fmaxf(fmaxf(l1, l2), 0.0f)), 0.0f);
+    return fmaxf(__fsub_rn(mn, fmax3f(l1, l2, 0.0f)), 0.0f);
 }
 
 }  // namespace ldpcb200
