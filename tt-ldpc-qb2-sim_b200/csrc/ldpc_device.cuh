@@ -91,11 +91,16 @@ __device__ __forceinline__ float amin_step(float m, float a) {
 // subtracts exactly one of c1, c2 or nothing, each with one rounding (a product with a 0/1 flag is
 // exact, and adding a signed zero leaves a value unchanged), so the result equals amin_step bit for
 // bit.  Inputs must be finite (c1 * 0 would be NaN for diff = inf): the QC kernel never feeds inf.
+// The product 0.328 (diff - 0.5) is one fused multiply-add, 0.328 diff - 0.164 with 0.164 exactly half
+// of the float 0.328: it rounds the exact value 0.328 (diff - 0.5) once, as the reference's
+// multiply does, because diff - 0.5 is exact for every diff in [0.25, 2) and c2 is used only on
+// [0.5, 2).
+constexpr float AMIN_K2 = 0.328f;
 __device__ __forceinline__ float amin_step_fma(float m, float a) {
     const float diff = fabsf(__fsub_rn(m, a));
     const float cur = fminf(m, a);
     const float c1 = __fsub_rn(0.69315f, __fmul_rn(0.40f, diff));
-    const float c2 = __fsub_rn(0.49315f, __fmul_rn(0.328f, __fsub_rn(diff, 0.5f)));
+    const float c2 = __fsub_rn(0.49315f, __fmaf_rn(AMIN_K2, diff, -0.5f * AMIN_K2));
     const float f05 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 536870912.0f));
     const float f2 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 2147483648.0f));
     const float t = __fmaf_rn(-c1, f05, cur);

@@ -394,14 +394,16 @@ template <int MODE> __device__ __forceinline__ void st_pair(typename LTraits<MOD
 
 // amin_step_fma on two independent lanes, its FMA-pipe arithmetic as packed f32x2 operations.
 // m, a >= 0 and finite.  diff = max(m,a) - min(m,a) is |m - a| exactly; c1n = 0.4 diff - 0.69315 and
-// c2n = 0.328 (diff - 0.5) - 0.49315 are the negated corrections (round-to-nearest is symmetric).
+// c2n = 0.328 (diff - 0.5) - 0.49315 are the negated corrections (round-to-nearest is symmetric;
+// the product as one fused multiply-add, as in amin_step_fma).
 __device__ __forceinline__ float2 amin_step_pair(float2 m, float2 a) {
     const float2 one = make_float2(1.0f, 1.0f), neg1 = make_float2(-1.0f, -1.0f);
     const float2 cur = make_float2(fminf(m.x, a.x), fminf(m.y, a.y));
     const float2 mx = make_float2(fmaxf(m.x, a.x), fmaxf(m.y, a.y));
     const float2 diff = __ffma2_rn(cur, neg1, mx);
     const float2 c1n = __ffma2_rn(__fmul2_rn(diff, make_float2(0.40f, 0.40f)), one, make_float2(-0.69315f, -0.69315f));
-    const float2 c2n = __ffma2_rn(__fmul2_rn(__fadd2_rn(diff, make_float2(-0.5f, -0.5f)), make_float2(0.328f, 0.328f)),
+    const float2 c2n = __ffma2_rn(__ffma2_rn(diff, make_float2(AMIN_K2, AMIN_K2),
+                                             make_float2(-0.5f * AMIN_K2, -0.5f * AMIN_K2)),
                                   one, make_float2(-0.49315f, -0.49315f));
     const float2 f05 = make_float2(__saturatef(__fmaf_rn(diff.x, -1073741824.0f, 536870912.0f)),
                                    __saturatef(__fmaf_rn(diff.y, -1073741824.0f, 536870912.0f)));
