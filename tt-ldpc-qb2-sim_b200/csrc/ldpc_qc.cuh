@@ -778,12 +778,17 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             if ((act >> f) & 1u)
                 if (it[f] >= (CIRC ? 1 : 3) || it[f] >= p.max_iter) eval |= 1u << f;
         if (!eval) continue;
-        if constexpr (!CIRC) {
-            // Pre-check: the sign parity of each thread's own rows in layers 0 and 2 (degree 3).  A frame
-            // with a failing row there has not converged, so unless it has reached max_iter it needs no
-            // ballots, syndrome words or counts this iteration.  These two layers show a failing row in
-            // about 97 % of the checks of frames that have not yet converged (2.5 to 3 dB).  A frame
-            // that passes goes through the full syndrome below, so the stop rule is unchanged.
+        {
+            // Pre-check: the sign parity of each thread's own rows in the two layers updated first in
+            // the iteration (layers 0 and 2 of degree 3; layers 4 and 6 of degree D in the circulant
+            // engine's order), or for the genie stop the sign bits of the info positions.  A frame
+            // failing it has not stopped, so unless it has reached max_iter it needs no ballots,
+            // syndrome words or counts this iteration.  Layers 0 and 2 show a failing row in about
+            // 97 % of the checks of frames that have not yet converged (2.5 to 3 dB).  A frame that
+            // passes goes through the full evaluation below, so the stop rule is unchanged.
+            const bool genie = CIRC && p.stop_rule == QC_STOP_GENIE;
+            constexpr int l0 = CIRC ? 4 : 0;
+            constexpr int dl = CIRC ? D : QC_DEG_LOW;
             uint32_t cand = 0;
 #pragma unroll
             for (int f = 0; f < F; ++f)
@@ -793,16 +798,20 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 if (!((cand >> f) & 1u)) continue;
                 const SV L(sL, f, lstride);
                 uint32_t bad = 0;
+                if (genie) {
+                    for (int i = tid; i < p.n_info; i += T) bad |= L.sign(i);
+                } else {
 #pragma unroll
-                for (int rho = 0; rho < R; ++rho) {
-                    const int j = tid + rho * T;
+                    for (int rho = 0; rho < R; ++rho) {
+                        const int j = tid + rho * T;
 #pragma unroll
-                    for (int l = 0; l < 4; l += 2) {
-                        uint32_t par = 0;
+                        for (int l = l0; l < l0 + 4; l += 2) {
+                            uint32_t par = 0;
 #pragma unroll
-                        for (int e = 0; e < QC_DEG_LOW; ++e)
-                            par ^= L.sign(p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1)));
-                        bad |= par;
+                            for (int e = 0; e < dl; ++e)
+                                par ^= L.sign(p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1)));
+                            bad |= par;
+                        }
                     }
                 }
                 if (__syncthreads_or((int)bad)) eval &= ~(1u << f);
