@@ -148,17 +148,21 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
             }
             ++it;
             if (it >= 3) {  // syndrome from iteration index 2 on (ldpc_decoder_core.h:526)
-                uint32_t bad = 0;
-                for (int m = lane; m < M && !bad; m += 32) {
+                // 32 rows at a time; the warp stops at the first group holding a failing row, so an
+                // unconverged frame usually costs a few groups instead of all M rows
+                bool bad = false;
+                for (int m0 = 0; m0 < M && !bad; m0 += 32) {
+                    const int m = m0 + lane;
                     uint32_t par = 0;
-                    for (int e = 0; e < p.dmax; ++e) {
-                        const int c = p.cols[e * M + m];
-                        if (c < 0) break;
-                        par ^= __float_as_uint(LT::ld(L, c)) >> 31;
-                    }
-                    bad |= par;
+                    if (m < M)
+                        for (int e = 0; e < p.dmax; ++e) {
+                            const int c = p.cols[e * M + m];
+                            if (c < 0) break;
+                            par ^= __float_as_uint(LT::ld(L, c)) >> 31;
+                        }
+                    bad = __any_sync(0xFFFFFFFFu, par) != 0;
                 }
-                if (!__any_sync(0xFFFFFFFFu, bad)) break;
+                if (!bad) break;
             }
         }
         // tally
