@@ -189,3 +189,26 @@ def test_circ_per_frame_snr_bins(dec_r12k1):
     assert int(bins[2].sum()) == r.bit_errors and int(bins[3].sum()) == r.iter_sum
     fer = bins[1][:8].sum() / max(1, bins[0][:8].sum()), bins[1][-8:].sum() / max(1, bins[0][-8:].sum())
     assert fer[0] > fer[1]
+
+
+def test_circ_cli(gpu, tmp_path, capsys):
+    """ldpc_sim --circulant: a short point on the makeH r1/2 K=1024 file ends with the final JSON
+    line; a matrix the decoder does not cover (rate 2/3) and an unbuilt storage fail cleanly."""
+    import io
+    import json
+
+    from ldpcb200 import sim
+    good = tmp_path / "r12.chinn.out"
+    good.write_text(ar4ja.make_code(1024, "1/2").chinn_out_text())
+    out = io.StringIO()
+    rc = sim.main(["-c", str(good), "-e", "1.5", "-p", "512", "-s", "-k", "20000", "-b", "10000", "-i", "50",
+                   "-t", "1000", "--circulant", "device"], out=out)
+    lines = [json.loads(l) for l in out.getvalue().splitlines() if l.startswith("{")]
+    assert rc == 0 and lines[-1]["blocks"] == 20000 and lines[-1]["frame_errors"] > 0
+    bad = tmp_path / "r23.chinn.out"
+    bad.write_text(ar4ja.make_code(1024, "2/3").chinn_out_text())
+    assert sim.main(["-c", str(bad), "-e", "2.0", "-p", "256", "-s", "-k", "100", "--circulant", "device"],
+                    out=io.StringIO()) == 1
+    assert sim.main(["-c", str(good), "-e", "2.0", "-p", "512", "-s", "-k", "100", "--circulant", "device",
+                     "--storage", "fp16"], out=io.StringIO()) == 1
+    assert "circulant engine's decoder cannot run" in capsys.readouterr().err

@@ -156,8 +156,14 @@ class GpuEngine:
         return "layered QC kernel" if self.dec.kind == self.capi.KERNEL_QC else "general file-order kernel"
 
     def set_circulant(self, o: Options):
+        """Settings of the circulant engine's decoder; raises if this matrix or storage has none
+        (rows of degrees 3 and 6 in the QC structure, a built storage mode)."""
         num, stop, damp = CIRC_MODES[o.circulant]
         self.dec.set_circulant(num, stop, damp if o.damping is None else o.damping)
+        # an empty chunk runs the parameter checks (QC structure, degrees, clips) without a launch
+        self.dec.run_chunk(self.dec.params(n_frames=0, max_iter=1, storage=o.storage, algo=self.capi.ALGO_CIRC))
+        if not self.dec.shapes(o.storage, self.capi.ALGO_CIRC):
+            raise ValueError(f"not built for --storage {o.storage} on this code")
 
     def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
         """For long runs of the QC kernel (Approximate-Min* or the circulant engine's decoder, no
