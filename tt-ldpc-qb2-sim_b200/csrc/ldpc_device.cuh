@@ -83,29 +83,26 @@ __device__ __forceinline__ float amin_step(float m, float a) {
     return fmaxf(__fsub_rn(cur, corr), 0.0f);
 }
 
-// The same step with the piecewise correction selected by FMA-pipe arithmetic instead of compares
-// and selects (the ALU pipe runs at half the FMA pipe's rate).  Flags f05 = [diff < 0.5] and
-// f2 = [diff < 2] come from saturated fused multiply-adds: 2^30 (0.5 - diff) is >= 32 for every float
-// diff below 0.5 and <= 0 otherwise, so saturation gives exactly 1 or 0.  Then
-//   t = cur - c1*f05,  u = t - c2*(f2 - f05)
-// subtracts exactly one of c1, c2 or nothing, each with one rounding (a product with a 0/1 flag is
+// The same step in 11 instructions.  The flag f2 = [diff < 2] comes from a saturated fused
+// multiply-add: 2^30 (2 - diff) is >= 32 for every float diff below 2 and <= 0 otherwise, so
+// saturation gives exactly 1 or 0.  With c the correction line of the region (c1 below 0.5, c2 from
+// there on), u = cur - c * f2 subtracts c with one rounding or nothing (a product with a 0/1 flag is
 // exact, and adding a signed zero leaves a value unchanged), so the result equals amin_step bit for
-// bit.  Inputs must be finite (c1 * 0 would be NaN for diff = inf): the QC kernel never feeds inf.
+// bit.  Inputs must be finite (c * 0 would be NaN for diff = inf): the QC kernel never feeds inf.
 // The product 0.328 (diff - 0.5) is one fused multiply-add, 0.328 diff - 0.164 with 0.164 exactly half
 // of the float 0.328: it rounds the exact value 0.328 (diff - 0.5) once, as the reference's
 // multiply does, because diff - 0.5 is exact for every diff in [0.25, 2) and c2 is used only on
-// [0.5, 2).
+// [0.5, 2).  (An earlier form selected both lines with two saturated flags, all on the FMA pipe: one
+// more instruction per step and 6 % slower, although it kept the busier ALU pipe free.)
 constexpr float AMIN_K2 = 0.328f;
 __device__ __forceinline__ float amin_step_fma(float m, float a) {
     const float diff = fabsf(__fsub_rn(m, a));
     const float cur = fminf(m, a);
     const float c1 = __fsub_rn(0.69315f, __fmul_rn(0.40f, diff));
     const float c2 = __fsub_rn(0.49315f, __fmaf_rn(AMIN_K2, diff, -0.5f * AMIN_K2));
-    const float f05 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 536870912.0f));
     const float f2 = __saturatef(__fmaf_rn(diff, -1073741824.0f, 2147483648.0f));
-    const float t = __fmaf_rn(-c1, f05, cur);
-    const float u = __fmaf_rn(-c2, __fsub_rn(f2, f05), t);
-    return fmaxf(u, 0.0f);
+    const float c = diff < 0.5f ? c1 : c2;
+    return fmaxf(__fmaf_rn(-c, f2, cur), 0.0f);
 }
 
 // The circulant engine's min* (tests/test_circulant_dma_stepper.cpp:39-54 and

@@ -392,8 +392,10 @@ template <int MODE> __device__ __forceinline__ void st_pair(typename LTraits<MOD
     }
 }
 
-// amin_step_fma on two independent lanes, its FMA-pipe arithmetic as packed f32x2 operations.
-// m, a >= 0 and finite.  diff = max(m,a) - min(m,a) is |m - a| exactly; c1n = 0.4 diff - 0.69315 and
+// amin_step_fma's result on two independent lanes, with the correction chosen by two saturated
+// flags, f05 = [diff < 0.5] and f2 = [diff < 2], so that every operation but the flags is a packed
+// f32x2 instruction: t = cur - c1 f05, u = t - c2 (f2 - f05), each subtracting c1, c2 or nothing
+// exactly once.  m, a >= 0 and finite.  diff = max(m,a) - min(m,a) is |m - a| exactly; c1n = 0.4 diff - 0.69315 and
 // c2n = 0.328 (diff - 0.5) - 0.49315 are the negated corrections (round-to-nearest is symmetric;
 // the product as one fused multiply-add, as in amin_step_fma).
 __device__ __forceinline__ float2 amin_step_pair(float2 m, float2 a) {
