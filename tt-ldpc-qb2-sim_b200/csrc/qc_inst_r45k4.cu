@@ -27,5 +27,10 @@ static const QcEntry qc_r45k4[] = {
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_BF16, ALGO_WAMIN, false, false, 0),
+    // check messages in global memory (layout 1): the 156 per-thread message registers of the
+    // register layout leave room for only 8-10 warps per SM; without them the kernel holds more frames
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
 };
 LDPC_QC_REGISTER(qc_r45k4)
