@@ -280,6 +280,28 @@ def test_offset_table_layout_equals_default_on_every_code(gpu, K, rate):
                     assert getattr(r, k) == getattr(base, k), (st, sh, k)
 
 
+@pytest.mark.parametrize("rate", ["2/3", "4/5"])
+def test_register_capped_k16384_shapes_equal_default(gpu, rate):
+    """The register-capped global-message shapes of the K = 16384 codes (two CTAs per SM) tally
+    exactly what the default shape tallies on the same frames."""
+    from ldpcb200 import threshold
+    c = ar4ja.make_code(16384, rate)
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db(rate) + 0.5)
+    with capi.Decoder.from_code(c, 0) as dec:
+        for st in ("bf16", "fp16"):
+            shapes = dec.shapes(st)
+            assert any(sh[2] == 2 for sh in shapes)
+            p = dec.params(mu=mu, sigma=sigma, seed=4, n_frames=600, max_iter=60, storage=st)
+            base = dec.run_chunk(p)
+            for sh in shapes:
+                dec.set_launch_shape(*sh, storage=st)
+                r = dec.run_chunk(p)
+                dec.set_launch_shape(0, 0, 0, 0, storage=st)
+                for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters",
+                          "bit_errors_sq"):
+                    assert getattr(r, k) == getattr(base, k), (st, sh, k)
+
+
 @pytest.mark.parametrize("ebn0", [0.0, 2.0, 4.0, 6.0, 8.0])
 def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
     """With no decoding iterations the tallies count the channel's own hard-decision errors: BPSK

@@ -20,5 +20,10 @@ static const QcEntry qc_k16[] = {
     K16_SHAPE(2048, 6, 4),
     K16_SHAPE(1024, 10, 2),
     K16_SHAPE(512, 18, 1),
+    // register cap of 64 (2 CTAs of 512 threads per SM) for the codes whose kernels need 77-110
+    LDPC_QC_ENTRY_G(1024, 10, 2, 1, STORE_BF16, ALGO_AMIN, false, false, 2),
+    LDPC_QC_ENTRY_G(1024, 10, 2, 1, STORE_FP16, ALGO_AMIN, false, false, 2),
+    LDPC_QC_ENTRY_G(512, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 2),
+    LDPC_QC_ENTRY_G(512, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 2),
 };
 LDPC_QC_REGISTER(qc_k16)
