@@ -38,17 +38,27 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
     int am = 0;
     float mag_min, mag_all;
     if (ALGO == ALGO_AMIN) {
-        float mn = 9999.0f;
+        // As the QC kernel's row update: prefix minima pm_i = min(9999, |q_0|, .., |q_i|), the
+        // argmin am = the first i with |q_i| = pm_{DT-1} (lt[i] = i < am), and the recursive min* over
+        // the other edges in row order, o_i = |q_i| for i < am and |q_{i+1}| after it
+        // (ldpc_decoder_core.h:414-475).  Edges past the row's degree are +inf: never the minimum,
+        // and a min* step with +inf leaves its value unchanged (amin_step), so the row runs
+        // DT - 1 steps whatever its degree.
+        float a[DT], pm[DT];
 #pragma unroll
-        for (int e = 0; e < DT; ++e)
-            if (e < deg) {
-                const float a = fabsf(q[e]);
-                if (a < mn) { mn = a; am = e; }
-            }
-        float mo = __int_as_float(0x7f800000);
+        for (int e = 0; e < DT; ++e) a[e] = e < deg ? fabsf(q[e]) : __int_as_float(0x7f800000);
+        pm[0] = fminf(a[0], 9999.0f);
 #pragma unroll
-        for (int e = 0; e < DT; ++e)
-            if (e < deg && e != am) mo = amin_step(mo, fabsf(q[e]));
+        for (int e = 1; e < DT; ++e) pm[e] = fminf(pm[e - 1], a[e]);
+        const float mn = pm[DT - 1];
+        bool lt[DT];
+#pragma unroll
+        for (int i = 0; i < DT; ++i) lt[i] = (i + 1 < DT) ? (pm[i] > mn) : false;
+#pragma unroll
+        for (int i = 0; i < DT; ++i) am += lt[i] ? 1 : 0;
+        float mo = DT > 1 ? (lt[0] ? a[0] : a[1]) : mn;
+#pragma unroll
+        for (int i = 1; i + 1 < DT; ++i) mo = amin_step(mo, lt[i] ? a[i] : a[i + 1]);
         if (deg == 1) mo = mn;  // m_others = min_mag when the row has one edge (:181)
         mag_min = mo;
         mag_all = amin_step(mo, mn);
@@ -252,7 +262,7 @@ int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCod
     }
     runs.push_back(M);
     g->n_runs = (int)runs.size() - 1;
-    g->dt = maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : maxdeg <= 32 ? 32 : 0;
+    g->dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : maxdeg <= 32 ? 32 : 0;
     if (!g->dt) return gfail(err, LDPC_ENOTSUP, "row degree above 32 is not supported");
     if (cudaMalloc(&g->d_cols, cols.size() * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&g->d_runs, runs.size() * sizeof(int32_t)) != cudaSuccess) {
@@ -299,10 +309,12 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
     // four frame slots per CTA while their L arrays fit comfortably in shared memory, else one
     const int nw = (size_t)GEN_WARPS * ((g->N + 7) & ~7) * esz <= 160 * 1024 ? GEN_WARPS : 1;
-    const void* fn = nw == GEN_WARPS ? (g->dt == 8    ? pick_mode<8>(p->storage, p->algo, ext)
+    const void* fn = nw == GEN_WARPS ? (g->dt == 6    ? pick_mode<6>(p->storage, p->algo, ext)
+                                        : g->dt == 8  ? pick_mode<8>(p->storage, p->algo, ext)
                                         : g->dt == 20 ? pick_mode<20>(p->storage, p->algo, ext)
                                                       : pick_mode<32>(p->storage, p->algo, ext))
-                                     : (g->dt == 8    ? pick_mode<8, 1>(p->storage, p->algo, ext)
+                                     : (g->dt == 6    ? pick_mode<6, 1>(p->storage, p->algo, ext)
+                                        : g->dt == 8  ? pick_mode<8, 1>(p->storage, p->algo, ext)
                                         : g->dt == 20 ? pick_mode<20, 1>(p->storage, p->algo, ext)
                                                       : pick_mode<32, 1>(p->storage, p->algo, ext));
     const size_t smem = (size_t)nw * ((g->N + 7) & ~7) * esz;
@@ -462,7 +474,7 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         if (c < -1 || c >= N) return sfail(LDPC_EINVAL, err, "edge index out of bounds");
         if (c >= 0) maxdeg = std::max(maxdeg, (int)(i % dmax) + 1);
     }
-    const int dt = maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : 32;
+    const int dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : 32;
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
     const size_t rsz = p->storage == STORE_FP32 ? 4 : 2;
     const size_t off_rows = 256;
@@ -497,7 +509,8 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         }
         base = g_static_addr[dev];
     }
-    const void* fn = dt == 8 ? pick_mode<8>(p->storage, p->algo, true)
+    const void* fn = dt == 6 ? pick_mode<6>(p->storage, p->algo, true)
+                   : dt == 8 ? pick_mode<8>(p->storage, p->algo, true)
                    : dt == 20 ? pick_mode<20>(p->storage, p->algo, true)
                               : pick_mode<32>(p->storage, p->algo, true);
     const size_t smem = (size_t)GEN_WARPS * ((N + 7) & ~7) * esz;
