@@ -41,12 +41,13 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
         // As the QC kernel's row update: prefix minima pm_i = min(9999, |q_0|, .., |q_i|), the
         // argmin am = the first i with |q_i| = pm_{DT-1} (lt[i] = i < am), and the recursive min* over
         // the other edges in row order, o_i = |q_i| for i < am and |q_{i+1}| after it
-        // (ldpc_decoder_core.h:414-475).  Edges past the row's degree are +inf: never the minimum,
-        // and a min* step with +inf leaves its value unchanged (amin_step), so the row runs
-        // DT - 1 steps whatever its degree.
+        // (ldpc_decoder_core.h:414-475).  Edges past the row's degree are the largest float: never
+        // the minimum, and a min* step with it leaves its value unchanged (diff >= 2, so nothing is
+        // subtracted, and every intermediate stays finite), so the row runs DT - 1 steps whatever its
+        // degree.
         float a[DT], pm[DT];
 #pragma unroll
-        for (int e = 0; e < DT; ++e) a[e] = e < deg ? fabsf(q[e]) : __int_as_float(0x7f800000);
+        for (int e = 0; e < DT; ++e) a[e] = e < deg ? fabsf(q[e]) : 3.40282347e38f;
         pm[0] = fminf(a[0], 9999.0f);
 #pragma unroll
         for (int e = 1; e < DT; ++e) pm[e] = fminf(pm[e - 1], a[e]);
@@ -58,10 +59,10 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
         for (int i = 0; i < DT; ++i) am += lt[i] ? 1 : 0;
         float mo = DT > 1 ? (lt[0] ? a[0] : a[1]) : mn;
 #pragma unroll
-        for (int i = 1; i + 1 < DT; ++i) mo = amin_step(mo, lt[i] ? a[i] : a[i + 1]);
+        for (int i = 1; i + 1 < DT; ++i) mo = amin_step_fma(mo, lt[i] ? a[i] : a[i + 1]);
         if (deg == 1) mo = mn;  // m_others = min_mag when the row has one edge (:181)
         mag_min = mo;
-        mag_all = amin_step(mo, mn);
+        mag_all = amin_step_fma(mo, mn);
     } else {
         float m1 = 999.0f, m2 = 999.0f;
 #pragma unroll

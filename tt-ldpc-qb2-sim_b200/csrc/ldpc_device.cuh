@@ -70,9 +70,9 @@ __device__ __forceinline__ float fp16_round_sat(float x) {  // IEEE fp16 RNE, sa
 }
 
 // ------------------------------------------------------------------ Approximate-Min*
-// min*(m, a) = max(min(m, a) - g(|m - a|), 0), g piecewise linear (ldpc_decoder_core.h:186-190).
-// With m = +inf the step returns a exactly, which lets the chain start from +inf instead of from the
-// first non-argmin edge (the reference's m_others = |q[first]|, :180-181).
+// min*(m, a) = max(min(m, a) - g(|m - a|), 0), g piecewise linear (ldpc_decoder_core.h:186-190),
+// stated as the reference writes it.  The kernels use amin_step_fma below, which returns the same
+// bits for finite inputs in fewer instructions.
 __device__ __forceinline__ float amin_step(float m, float a) {
     const float diff = fabsf(__fsub_rn(m, a));
     const float cur = fminf(m, a);
