@@ -96,7 +96,9 @@ typedef struct {
     uint64_t iter_sum;     /* executed iterations, including the one that met the syndrome */
     uint64_t unconverged;  /* frames whose syndrome still fails after decoding */
     uint64_t max_iters;    /* largest iteration count of one frame */
-    float kernel_ms;       /* device time of the decode kernel (CUDA events on the handle's stream) */
+    float kernel_ms;       /* device time of the decode kernel (CUDA events on the handle's stream;
+                              for a large ldpc_decode_llr, from the first launch to the end of the
+                              last, waits for later chunks' LLR copies included) */
     float reserved1;
     uint64_t bit_errors_sq; /* sum over frames of (bit errors of the frame)^2: the frame-level variance
                                of the bit-error count, for confidence intervals on BER */
@@ -118,7 +120,9 @@ int ldpc_kernel_kind(const ldpc_handle* h);
  * the tallies are on the host. */
 int ldpc_run_chunk(ldpc_handle* h, const ldpc_run_params* p, ldpc_tally* out);
 
-/* Decodes n_frames caller-supplied frames: llr [n_frames][N-P] fp32 channel LLRs (host).  Uses
+/* Decodes n_frames caller-supplied frames: llr [n_frames][N-P] fp32 channel LLRs (host; pinned
+ * memory copies fastest, and from 16384 frames on the copy of each chunk of frames overlaps the
+ * decoding of the previous one).  Uses
  * p->max_iter, storage, algo and the clips (mu/sigma/seed ignored).  Outputs (each may be NULL):
  * post [n_frames][N] final L as stored (bf16/fp16 values widened to float), iters, synd_fail (rows
  * failing after decoding), bit_errors. */

@@ -280,6 +280,24 @@ def test_offset_table_layout_equals_default_on_every_code(gpu, K, rate):
                     assert getattr(r, k) == getattr(base, k), (st, sh, k)
 
 
+def test_large_decode_llr_pipelined_copy(dec_r12k1):
+    """From 16384 frames on, ldpc_decode_llr copies the LLRs in chunks on a second stream while the
+    previous chunk decodes: the results equal the fused simulation of the same channel and, frame by
+    frame, a small (unpipelined) call on a slice."""
+    c = ar4ja.make_code(1024, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.5)
+    p = dec_r12k1.params(mu=mu, sigma=sigma, seed=91, n_frames=40000, max_iter=100, storage="fp32")
+    sim = dec_r12k1.run_chunk(p)
+    llr = dec_r12k1.channel_llr(p)
+    post, it, sf, be, tal = dec_r12k1.decode_llr(llr, p, want_post=False)
+    assert (tal.frames, tal.bit_errors, tal.frame_errors, tal.iter_sum, tal.bit_errors_sq) == \
+           (sim.frames, sim.bit_errors, sim.frame_errors, sim.iter_sum, sim.bit_errors_sq)
+    _check_tally(tal, it, sf, be)
+    sl = slice(17000, 23000)  # spans a chunk boundary
+    _, it2, sf2, be2, _ = dec_r12k1.decode_llr(llr[sl], p, want_post=False)
+    assert np.array_equal(it[sl], it2) and np.array_equal(sf[sl], sf2) and np.array_equal(be[sl], be2)
+
+
 @pytest.mark.parametrize("rate", ["2/3", "4/5"])
 def test_register_capped_k16384_shapes_equal_default(gpu, rate):
     """The register-capped global-message shapes of the K = 16384 codes (two CTAs per SM) tally

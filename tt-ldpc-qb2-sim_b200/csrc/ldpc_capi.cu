@@ -97,6 +97,10 @@ struct ldpc_handle {
     ldpc_circ_config circ{LDPC_CIRC_SFPU, LDPC_CIRC_STOP_GENIE, 0.9375f, 0};
     unsigned long long* h_tally = nullptr;  // pinned
     int64_t launches = 0;
+    // ldpc_decode_llr: a copy stream and an event that let the decoding of one chunk of frames
+    // overlap the host->device copy of the next (created on first use)
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t cev = nullptr;
 };
 
 static int detect_qc(ldpc_handle* h) {
@@ -181,6 +185,8 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     if (h->h_tally) cudaFreeHost(h->h_tally);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->cev) cudaEventDestroy(h->cev);
+    if (h->cstream) cudaStreamDestroy(h->cstream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -577,14 +583,24 @@ static int read_tally(ldpc_handle* h, ldpc_tally* out) {
 // Splits a request into launches of at most 2^31 frames (the kernel's claim counter is 32-bit).
 static constexpr uint64_t kMaxLaunchFrames = 1ull << 31;
 
+// h_llr (host, optional): the channel LLRs of the n frames, copied into d_llr one chunk at a time on
+// the handle's copy stream while the previous chunk decodes; chunk <= kMaxLaunchFrames.
 static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64_t n, const float* d_llr,
-                      float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be) {
+                      float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be, const float* h_llr = nullptr,
+                      uint64_t chunk = kMaxLaunchFrames) {
     int rc;
     if ((rc = reset_counters(h))) return rc;
-    CU(cudaEventRecord(h->ev0, h->stream));
-    for (uint64_t off = 0; off < n || (n == 0 && off == 0); off += kMaxLaunchFrames) {
-        if (n == 0) break;
-        const uint32_t cnt = (uint32_t)std::min<uint64_t>(kMaxLaunchFrames, n - off);
+    if (n == 0) CU(cudaEventRecord(h->ev0, h->stream));
+    const uint64_t ntx = (uint64_t)(h->N - h->P);
+    for (uint64_t off = 0; off < n; off += chunk) {
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(chunk, n - off);
+        if (h_llr) {
+            CU(cudaMemcpyAsync(const_cast<float*>(d_llr) + off * ntx, h_llr + off * ntx, cnt * ntx * sizeof(float),
+                               cudaMemcpyHostToDevice, h->cstream));
+            CU(cudaEventRecord(h->cev, h->cstream));
+            CU(cudaStreamWaitEvent(h->stream, h->cev, 0));
+        }
+        if (off == 0) CU(cudaEventRecord(h->ev0, h->stream));
         if (off) CU(cudaMemsetAsync(h->d_work, 0, 64, h->stream));
         const float* llr = d_llr ? d_llr + off * (uint64_t)(h->N - h->P) : nullptr;
         float* post = d_post ? d_post + off * (uint64_t)h->N : nullptr;
@@ -637,6 +653,19 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
         if ((rc = ensure_cap((void**)&h->d_llr, &h->llr_cap, nb * ntx * sizeof(float)))) return rc;
         if (post && (rc = ensure_cap((void**)&h->d_post, &h->post_cap, nb * h->N * sizeof(float)))) return rc;
         if ((rc = ensure_cap((void**)&h->d_frame_out, &h->frame_cap, 3 * nb * sizeof(int32_t)))) return rc;
+    }
+    // Large calls copy the LLRs in chunks on a second stream, so that the decoding of one chunk
+    // overlaps the copy of the next; small ones copy everything first.
+    constexpr uint64_t kMinChunk = 8192;
+    const bool pipelined = nb >= 2 * kMinChunk;
+    uint64_t chunk = kMaxLaunchFrames;
+    if (pipelined) {
+        if (!h->cstream && cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(LDPC_EIO, "copy stream creation failed");
+        if (!h->cev && cudaEventCreateWithFlags(&h->cev, cudaEventDisableTiming) != cudaSuccess)
+            return fail(LDPC_EIO, "copy event creation failed");
+        chunk = std::min<uint64_t>(kMaxLaunchFrames, std::max<uint64_t>(kMinChunk, (nb + 7) / 8));
+    } else if (nb) {
         CU(cudaMemcpyAsync(h->d_llr, llr, nb * ntx * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     }
     ldpc_run_params q = *p;
@@ -645,7 +674,9 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
     int32_t* d_it = h->d_frame_out;
     int32_t* d_sf = d_it ? d_it + nb : nullptr;
     int32_t* d_be = d_sf ? d_sf + nb : nullptr;
-    if ((rc = run_frames(h, &q, true, nb, h->d_llr, post ? h->d_post : nullptr, d_it, d_sf, d_be))) return rc;
+    if ((rc = run_frames(h, &q, true, nb, h->d_llr, post ? h->d_post : nullptr, d_it, d_sf, d_be,
+                         pipelined ? llr : nullptr, chunk)))
+        return rc;
     if (nb) {
         if (post) CU(cudaMemcpyAsync(post, h->d_post, nb * h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
         if (iters) CU(cudaMemcpyAsync(iters, d_it, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
