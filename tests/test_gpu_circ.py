@@ -212,3 +212,24 @@ def test_circ_cli(gpu, tmp_path, capsys):
     assert sim.main(["-c", str(good), "-e", "2.0", "-p", "512", "-s", "-k", "100", "--circulant", "device",
                      "--storage", "fp16"], out=io.StringIO()) == 1
     assert "circulant engine's decoder cannot run" in capsys.readouterr().err
+
+
+def test_circ_fer_matches_reference_stepper_monte_carlo(dec_r12k1):
+    """Statistical parity with the reference's own circulant Monte Carlo (its stepper's scalar path,
+    its std::normal_distribution channel; tests/golden/fer_reference_circulant.json, made by
+    tests/golden/make_fer_reference_circ.py): at every Eb/N0 point the 95% Clopper-Pearson intervals
+    of the frame error rates overlap.  The GPU decodes 10^5 Philox frames per point with the same
+    settings (scalar arithmetic, syndrome after every iteration, no damping, 200 iterations)."""
+    import json
+
+    from ldpcb200 import stats
+    ref = json.load(open(os.path.join(os.path.dirname(GOLDEN), "fer_reference_circulant.json")))
+    d = dec_r12k1
+    d.set_circulant(capi.CIRC_SCALAR, capi.CIRC_STOP_SYNDROME, 1.0)
+    for pt in ref["points"]:
+        mu, sigma = capi.channel_mu_sigma(d.N, d.M, d.P, pt["ebn0"])
+        r = d.run_chunk(d.params(mu=mu, sigma=sigma, seed=5, n_frames=100000, max_iter=200, storage="bf16",
+                                 algo=capi.ALGO_CIRC))
+        ours = stats.clopper_pearson(r.frame_errors, r.frames)
+        theirs = stats.clopper_pearson(pt["frame_errors"], pt["frames"])
+        assert stats.intervals_overlap(ours, theirs), (pt["ebn0"], r.frame_errors, pt["frame_errors"])
