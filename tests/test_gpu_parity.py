@@ -298,6 +298,26 @@ def test_large_decode_llr_pipelined_copy(dec_r12k1):
     assert np.array_equal(it[sl], it2) and np.array_equal(sf[sl], sf2) and np.array_equal(be[sl], be2)
 
 
+@pytest.mark.parametrize("K", [1024, 4096])
+def test_degree18_fp32_global_messages_equal_general_kernel(gpu, K):
+    """fp32 storage of the rate-4/5 codes simulates on the global-message QC kernel (its only fp32
+    layout) and decodes caller LLRs on the general kernel: the simulation's tallies equal decoding
+    its own exported channel."""
+    from ldpcb200 import threshold
+    c = ar4ja.make_code(K, "4/5")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db("4/5") + (0.5 if K == 1024 else 0.2))
+    with capi.Decoder.from_code(c, 0) as dec:
+        assert (1, 1, 0, 1) in dec.shapes("fp32")
+        p = dec.params(mu=mu, sigma=sigma, seed=12, n_frames=1000 if K == 1024 else 300, max_iter=60,
+                       storage="fp32")
+        sim = dec.run_chunk(p)
+        llr = dec.channel_llr(p)
+        _, it, sf, be, tal = dec.decode_llr(llr, p, want_post=False)
+    assert (sim.frames, sim.bit_errors, sim.frame_errors, sim.iter_sum, sim.unconverged, sim.bit_errors_sq) == \
+           (tal.frames, tal.bit_errors, tal.frame_errors, tal.iter_sum, tal.unconverged, tal.bit_errors_sq)
+    assert sim.frame_errors > 0
+
+
 @pytest.mark.parametrize("rate", ["2/3", "4/5"])
 def test_register_capped_k16384_shapes_equal_default(gpu, rate):
     """The register-capped global-message shapes of the K = 16384 codes (two CTAs per SM) tally
