@@ -285,6 +285,17 @@ static inline float circ_g(const circ_consts* k, float a, float b) {
     return (v < 0.0f) ? 0.0f : v;
 }
 
+/* The min* alone on n pairs ab[2i], ab[2i+1] (numerics as above), for pinning it to the
+ * reference's min* unit test (tests/unit_sfpu/test_piecewise_amin_star.cpp:44-53). */
+void oracle_circ_g_n(int numerics, const float* ab, int n, float* out) {
+    circ_consts k = {0.69315f, -0.40f, 0.65715f, -0.328f};
+    if (numerics == CIRC_SFPU) {
+        k.c1 = trunc_bf16(k.c1); k.k1 = trunc_bf16(k.k1);
+        k.c2 = trunc_bf16(k.c2); k.k2 = trunc_bf16(k.k2);
+    }
+    for (int i = 0; i < n; i++) out[i] = circ_g(&k, ab[2 * i], ab[2 * i + 1]);
+}
+
 static int syndrome_failures_lt0(int M, int dmax, const int32_t* rows, const int32_t* degs, const float* L) {
     int fails = 0;
     for (int m = 0; m < M; m++) {

@@ -63,6 +63,8 @@ def lib():
                                          C.c_int, P(C.c_float), P(C.c_float), P(C.c_float),
                                          P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int32)]
         L.oracle_circ_decode.restype = C.c_int
+        L.oracle_circ_g_n.argtypes = [C.c_int, P(C.c_float), C.c_int, P(C.c_float)]
+        L.oracle_circ_g_n.restype = None
         _lib = L
     return _lib
 
@@ -149,6 +151,14 @@ def circ_decode(code: Code, llr: np.ndarray, numerics: int = CIRC_SFPU, damping:
             raise ValueError("oracle_circ_decode rejected its arguments")
         out[:, i] = [x.value for x in v]
     return post, out[0], out[1], out[2], out[3]
+
+
+def circ_g(numerics: int, a, b) -> np.ndarray:
+    """The circulant engine's min* of the oracle on arrays a, b (float32)."""
+    ab = np.ascontiguousarray(np.stack([np.asarray(a, np.float32), np.asarray(b, np.float32)], axis=-1).ravel())
+    out = np.zeros(ab.size // 2, np.float32)
+    lib().oracle_circ_g_n(numerics, _p(ab, C.c_float), out.size, _p(out, C.c_float))
+    return out
 
 
 def philox4x32_10(ctr, key) -> np.ndarray:
@@ -297,3 +307,22 @@ def run_ref_circ(llr_bf16_bits: np.ndarray, sfpu: bool, damping: float, max_iter
         active[4 * g:4 * g + 4] = tail[4:8]
         be[4 * g:4 * g + 4] = tail[8:12]
     return post, iters, active, be
+
+
+def run_ref_gdelta(a, b):
+    """The reference's min* unit test function approx_min_star_2piece (oracle/_ref/ref_gdelta) on
+    pairs: (plain float32 results, bf16-rounded results)."""
+    exe = ref_binary("ref_gdelta")
+    if exe is None:
+        raise FileNotFoundError("oracle/_ref/ref_gdelta is not built (make -C oracle ref)")
+    ab = np.ascontiguousarray(np.stack([np.asarray(a, np.float32), np.asarray(b, np.float32)], axis=-1).ravel())
+    n = ab.size // 2
+    with tempfile.TemporaryDirectory() as td:
+        ip = os.path.join(td, "in.bin")
+        op = os.path.join(td, "out.bin")
+        with open(ip, "wb") as f:
+            f.write(np.uint32(n).tobytes())
+            f.write(ab.tobytes())
+        subprocess.run([exe, ip, op], check=True)
+        out = np.fromfile(op, dtype=np.float32)
+    return out[:n], out[n:]

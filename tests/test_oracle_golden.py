@@ -172,3 +172,18 @@ def test_circ_oracle_rejects_bad_arguments():
     for damp in (0.0, 1.5, float("nan")):
         with pytest.raises(ValueError):
             O.circ_decode(code12, np.zeros((1, 2048), np.float32), damping=damp, max_iter=1)
+
+
+def test_circ_min_star_matches_reference_unit_test():
+    """The oracle's two-line min* (the circulant engine's, exact constants) against the reference's
+    own min* unit test function approx_min_star_2piece (tests/unit_sfpu/test_piecewise_amin_star.cpp,
+    tests/golden/golden_gdelta.npz): its sweep, region-edge corner cases and random pairs, bit for
+    bit; the bf16-rounded outputs of the test equal the rounded oracle values."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_gdelta.npz"))
+    g = O.circ_g(O.CIRC_SCALAR, z["a"], z["b"])
+    assert np.array_equal(g.view(np.uint32), z["out"].view(np.uint32))
+    assert np.array_equal(_f32_to_bf16_bits(g), (z["out_bf16"].view(np.uint32) >> 16).astype(np.uint16))
+    # the SFPU form (bf16-truncated constants) is a different function: it differs on most pairs
+    s = O.circ_g(O.CIRC_SFPU, z["a"], z["b"])
+    assert (s.view(np.uint32) != g.view(np.uint32)).mean() > 0.3
