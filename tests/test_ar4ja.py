@@ -129,3 +129,45 @@ def test_shipped_matrix_is_the_same_code_up_to_order(golden):
     m = chinn.Matrix(N=2560, M=1536, max_var_deg=6, max_check_deg=6, rows=[r[r >= 0] for r in rows])
     assert chinn.match_ar4ja(m) is None
     assert len(chinn.conflict_free_runs(m)) - 1 == 135
+
+
+def test_circulant_tile_slices_decode_exactly_h():
+    """The circulant engine gathers every edge of 16 consecutive checks as one or two contiguous runs
+    of variable nodes (TILE_SLICES_*, engines/circulant_dma_4cw/ar4ja_circulant_descriptors_4cw.h):
+    tiles 0-31 hold rows 512..1535 (32 checks, edges 0-2 in faces 0/1, 3-5 in faces 2/3), tiles 32-39
+    rows 0..511 (64 checks, one face per 16).  Reconstructed check by check, the gathered variables are
+    each row's columns in ascending order, so the engine decodes exactly H with that edge order and
+    tile schedule: the layout the GPU's circulant decoder (LDPC_ALGO_CIRC) assumes."""
+    path = os.path.join(REFERENCE, "engines", "circulant_dma_4cw", "ar4ja_circulant_descriptors_4cw.h")
+    if not os.path.exists(path):
+        pytest.skip("reference tree not present")
+    src = open(path).read()
+
+    def table(name):
+        body = src[src.index(name + "[40][3]"):]
+        body = body[:body.index("};")]
+        ent = re.findall(r"\{\s*0x([0-9A-Fa-f]+)u,\s*0x([0-9A-Fa-f]+)u,\s*(\d+)u,\s*(\d+)u", body)
+        assert len(ent) == 120
+        return [ent[3 * t:3 * t + 3] for t in range(40)]
+
+    def nodes(desc):
+        oa, ob, la, lb = int(desc[0], 16), int(desc[1], 16), int(desc[2]), int(desc[3])
+        out = [oa // 8 + i for i in range(la // 8)] + [ob // 8 + i for i in range(lb // 8)]
+        assert len(out) == 16
+        return out
+
+    f0, f2 = table("TILE_SLICES_W0_F0"), table("TILE_SLICES_W0_F2")
+    f1, f3 = table("TILE_SLICES_W1_F1"), table("TILE_SLICES_W1_F3")
+    rows = [list(r) for r in ar4ja.make_code(1024, "1/2").rows()]
+    for t in range(40):
+        if t < 32:  # worker 0: checks 0..15 (faces 0, 2), worker 1: checks 16..31 (faces 1, 3)
+            for w, (lo, hi) in enumerate(((f0, f2), (f1, f3))):
+                for c in range(16):
+                    m = 512 + 32 * t + 16 * w + c
+                    got = [nodes(lo[t][d])[c] for d in range(3)] + [nodes(hi[t][d])[c] for d in range(3)]
+                    assert got == rows[m], (t, m)
+        else:
+            for fi, face in enumerate((f0, f1, f2, f3)):
+                for c in range(16):
+                    m = 64 * (t - 32) + 16 * fi + c
+                    assert [nodes(face[t][d])[c] for d in range(3)] == rows[m], (t, m)
