@@ -23,13 +23,18 @@ enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2, ALGO_CIRC = 3 };
 // ------------------------------------------------------------------ Philox-4x32-10
 struct U32x4 { uint32_t x, y, z, w; };
 
+// One round: each 32x32-bit product is one wide multiply (both halves at once).
+__device__ __forceinline__ U32x4 philox_round(U32x4 c, uint32_t k0, uint32_t k1) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    return U32x4{(uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0};
+}
+
 __device__ __forceinline__ U32x4 philox4x32_10(U32x4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
         if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
-        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = U32x4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        c = philox_round(c, k0, k1);
     }
     return c;
 }
