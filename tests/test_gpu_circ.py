@@ -233,3 +233,30 @@ def test_circ_fer_matches_reference_stepper_monte_carlo(dec_r12k1):
         ours = stats.clopper_pearson(r.frame_errors, r.frames)
         theirs = stats.clopper_pearson(pt["frame_errors"], pt["frames"])
         assert stats.intervals_overlap(ours, theirs), (pt["ebn0"], r.frame_errors, pt["frame_errors"])
+
+
+def test_circulant_engine_binary_drop_in(gpu, tmp_path):
+    """ldpc_sim_circulant_dma (the drop-in for the reference's circulant engine binary): a short
+    single-core run writes the engine's CSV rows and summary, and its totals equal ldpc_run_chunk with
+    the same settings over the same frames."""
+    import io
+
+    from ldpcb200 import sim_circ
+    csv = tmp_path / "c.csv"
+    out = io.StringIO()
+    rc = sim_circ.main(["1.5", "30000", "50", "--single-core", "--chunk-batches", "2500", "--min-fe", "1000000",
+                        "--out", str(csv), "--seed", "17"], out=out)
+    assert rc == 0
+    rows = csv.read_text().splitlines()
+    assert len(rows) == 1 + 3  # header + chunks of 10000, 10000, 10000
+    blocks, be, fe = (int(x) for x in rows[-1].split(",")[1:4])
+    assert blocks == 30000 and fe > 0
+    c = ar4ja.make_code(1024, "1/2")
+    with capi.Decoder.from_code(c, 0) as dec:
+        dec.set_circulant(capi.CIRC_SFPU, capi.CIRC_STOP_GENIE, 0.9375)
+        g = 10.0 ** 0.15
+        p = dec.params(mu=float(np.float32(2.0 * g)), sigma=float(np.float32(np.sqrt(4.0 * g))), seed=17,
+                       n_frames=30000, max_iter=50, storage="bf16", algo=capi.ALGO_CIRC)
+        r = dec.run_chunk(p)
+    assert (r.frames, r.bit_errors, r.frame_errors) == (blocks, be, fe)
+    assert any(l.strip() == f"Frame Errors:     {fe}" for l in out.getvalue().splitlines())
