@@ -318,18 +318,21 @@ def test_degree18_fp32_global_messages_equal_general_kernel(gpu, K):
     assert sim.frame_errors > 0
 
 
-@pytest.mark.parametrize("rate", ["2/3", "4/5"])
-def test_register_capped_k16384_shapes_equal_default(gpu, rate):
-    """The register-capped global-message shapes of the K = 16384 codes (two CTAs per SM) tally
-    exactly what the default shape tallies on the same frames."""
+@pytest.mark.parametrize("K,rate,storages", [(16384, "2/3", ("bf16", "fp16")), (16384, "4/5", ("bf16", "fp16")),
+                                              (1024, "4/5", ("bf16", "fp16", "fp32")),
+                                              (4096, "4/5", ("bf16", "fp16", "fp32"))])
+def test_register_capped_global_message_shapes_equal_default(gpu, K, rate, storages):
+    """The register-capped global-message shapes (two CTAs per SM for K = 16384, 64 registers for
+    the degree-18 rate-4/5 codes) tally exactly what the default shape tallies on the same frames."""
     from ldpcb200 import threshold
-    c = ar4ja.make_code(16384, rate)
+    c = ar4ja.make_code(K, rate)
     mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db(rate) + 0.5)
     with capi.Decoder.from_code(c, 0) as dec:
-        for st in ("bf16", "fp16"):
+        for st in storages:
             shapes = dec.shapes(st)
-            assert any(sh[2] == 2 for sh in shapes)
-            p = dec.params(mu=mu, sigma=sigma, seed=4, n_frames=600, max_iter=60, storage=st)
+            assert any(sh[2] > 0 and sh[3] == 1 for sh in shapes), (st, shapes)
+            p = dec.params(mu=mu, sigma=sigma, seed=4, n_frames=600 if K == 16384 else 2000, max_iter=60,
+                           storage=st)
             base = dec.run_chunk(p)
             for sh in shapes:
                 dec.set_launch_shape(*sh, storage=st)

@@ -28,5 +28,9 @@ static const QcEntry qc_r45k1[] = {
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
+    // the same capped at 64 registers (32 CTAs of 32 threads per SM)
+    LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 32),
+    LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 32),
+    LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 32),
 };
 LDPC_QC_REGISTER(qc_r45k1)

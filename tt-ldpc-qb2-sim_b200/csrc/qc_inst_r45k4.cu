@@ -32,5 +32,9 @@ static const QcEntry qc_r45k4[] = {
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
+    // the same capped at 64 registers (8 CTAs of 128 threads per SM)
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 8),
 };
 LDPC_QC_REGISTER(qc_r45k4)
