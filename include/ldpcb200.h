@@ -48,7 +48,7 @@ extern "C" {
 
 /* Decoder family chosen for a matrix (ldpc_kernel_kind). */
 #define LDPC_KERNEL_QC 0      /* quasi-cyclic layered kernel (AR4JA structure detected) */
-#define LDPC_KERNEL_GENERAL 1 /* any matrix, rows in file order in conflict-free runs */
+#define LDPC_KERNEL_GENERAL 1 /* any matrix, file order kept where rows share a variable (ldpc_row_schedule) */
 
 typedef struct ldpc_handle ldpc_handle;
 
@@ -114,6 +114,16 @@ void ldpc_destroy(ldpc_handle* h);
 
 /* LDPC_KERNEL_QC or LDPC_KERNEL_GENERAL, or a negative error. */
 int ldpc_kernel_kind(const ldpc_handle* h);
+
+/* The row schedule the general kernel runs a matrix with (host only, needs no GPU).  The reference
+ * updates the rows one after another in file order (ldpc_decoder_core.h:314-522); rows that share no
+ * variable commute bit for bit, so the kernel runs the rows in steps of at most 32 rows sharing no
+ * variable, with every pair of rows that share one in file order: rows sorted by their earliest level
+ * (1 + the highest level among the earlier rows they share a variable with; file order inside a
+ * level), cut greedily into steps.  Writes the file rows in schedule order to order[M] and the first
+ * position of every step followed by M to starts[M + 1]; returns the number of steps, or a negative
+ * error for a bad matrix. */
+int ldpc_row_schedule(const ldpc_matrix* h, int32_t* order, int32_t* starts);
 
 /* Simulates p->n_frames frames (channel generation, decoding, tallies) on the device; replaces one
  * batch of ldpc_sim_scalar.cpp:421-589 (EnqueueMeshWorkload + ReadShard + host sums).  Blocks until

@@ -3,7 +3,6 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <unordered_set>
 #include <vector>
 
 #include "ldpc_general.cuh"
@@ -233,35 +232,77 @@ static int gfail(std::string& err, int code, const std::string& msg) {
     return code;
 }
 
+// The row schedule of the general kernel.  Two rows that share no variable commute: updating them
+// in either order, or at once, gives the same bits, because a row reads and writes only its own
+// variables' posteriors and its own messages.  So any order that keeps every pair of rows sharing a
+// variable in file order decodes exactly as the file order does.  Each row gets its earliest level,
+// 1 + the highest level among the earlier rows it shares a variable with; the rows sorted by level
+// (file order inside a level) are such an order, and the greedy cut of that order into steps of
+// consecutive rows sharing no variable, at most 32 rows each (one warp pass), gives the steps the
+// kernel runs with a warp barrier between them.  For the reference's shipped r1/2 K=1024 file (135
+// runs of consecutive conflict-free rows in file order, 11.4 rows on average) this gives 51 steps of
+// about 30 rows; for makeH order, Z/32 steps per layer as before.  `order` receives the file rows in
+// schedule order, `starts` the first position of every step followed by M.
+void general_schedule(const int32_t* rows, int N, int M, int dmax, std::vector<int32_t>& order,
+                      std::vector<int32_t>& starts) {
+    std::vector<int32_t> lev(M), last(N, 0);
+    int maxl = 0;
+    for (int m = 0; m < M; ++m) {
+        int l = 0;
+        for (int e = 0; e < dmax; ++e) {
+            const int32_t c = rows[(size_t)m * dmax + e];
+            if (c >= 0) l = std::max(l, last[c]);
+        }
+        lev[m] = ++l;
+        maxl = std::max(maxl, l);
+        for (int e = 0; e < dmax; ++e) {
+            const int32_t c = rows[(size_t)m * dmax + e];
+            if (c >= 0) last[c] = l;
+        }
+    }
+    std::vector<int32_t> pos(maxl + 2, 0);
+    for (int m = 0; m < M; ++m) ++pos[lev[m] + 1];
+    for (int l = 1; l <= maxl + 1; ++l) pos[l] += pos[l - 1];
+    order.assign(M, 0);
+    for (int m = 0; m < M; ++m) order[pos[lev[m]]++] = m;
+    starts.assign(1, 0);
+    std::vector<char> used(N, 0);
+    int start = 0;
+    for (int k = 0; k < M; ++k) {
+        const int32_t* rv = rows + (size_t)order[k] * dmax;
+        bool cut = k - start == 32;
+        for (int e = 0; e < dmax && !cut; ++e) cut = rv[e] >= 0 && used[rv[e]];
+        if (cut) {
+            starts.push_back(k);
+            for (int j = start; j < k; ++j)
+                for (int e = 0; e < dmax; ++e) {
+                    const int32_t c = rows[(size_t)order[j] * dmax + e];
+                    if (c >= 0) used[c] = 0;
+                }
+            start = k;
+        }
+        for (int e = 0; e < dmax; ++e)
+            if (rv[e] >= 0) used[rv[e]] = 1;
+    }
+    starts.push_back(M);
+}
+
 int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCode* g, std::string& err) {
     g->N = N;
     g->M = M;
     g->P = P;
     g->dmax = dmax;
     int maxdeg = 0;
+    std::vector<int32_t> order, runs;
+    general_schedule(rows, N, M, dmax, order, runs);
     std::vector<int32_t> cols((size_t)dmax * M, -1);
-    std::vector<int32_t> runs{0};
-    std::unordered_set<int32_t> used;
-    for (int m = 0; m < M; ++m) {
-        int d = 0;
-        std::vector<int32_t> rv;
+    for (int k = 0; k < M; ++k)
         for (int e = 0; e < dmax; ++e) {
-            const int32_t c = rows[(size_t)m * dmax + e];
+            const int32_t c = rows[(size_t)order[k] * dmax + e];
             if (c < 0) break;
-            cols[(size_t)e * M + m] = c;
-            rv.push_back(c);
-            d = e + 1;
+            cols[(size_t)e * M + k] = c;
+            maxdeg = std::max(maxdeg, e + 1);
         }
-        maxdeg = std::max(maxdeg, d);
-        bool clash = false;
-        for (int32_t c : rv) clash |= used.count(c) > 0;
-        if (clash) {
-            runs.push_back(m);
-            used.clear();
-        }
-        for (int32_t c : rv) used.insert(c);
-    }
-    runs.push_back(M);
     g->n_runs = (int)runs.size() - 1;
     g->dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : maxdeg <= 32 ? 32 : 0;
     if (!g->dt) return gfail(err, LDPC_ENOTSUP, "row degree above 32 is not supported");
@@ -398,8 +439,9 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
 //   [0, 256)           frame-claim counter (u32) and tallies (TALLY_WORDS x u64)
 //   rows               the caller's [M][dmax] row table, copied in
 //   cols               the same table transposed to [dmax][M] (the general kernel's layout)
-//   runs               conflict-free run starts (M + 1 entries) and their count
-//   bitmap             N bits, used while the runs are computed
+//   runs               step starts (M + 1 entries) and their count
+//   bitmap             N bits, used while the steps are cut
+//   lev, last, order, cnt   work space of the schedule: M, N, M and M + 2 ints
 //   messages           [slots][dmax][M] check messages, one region per frame slot
 // Every call rewrites the tables and zeroes the counter and tallies; the messages are zeroed by the
 // kernel when it starts a frame.  All calls share the one array, so calls whose work overlaps on the
@@ -415,27 +457,72 @@ unsigned char* g_static_addr[kMaxDevices] = {};
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Transposes the row table and splits the file row order into conflict-free runs (the same greedy
-// rule as build_general), one warp, no waits on other threads.
+// The schedule of general_schedule on the device (the same levels, order and steps), one warp, no
+// waits on other threads: the caller's [M][dmax] row table in, the [dmax][M] table in schedule order
+// and the step starts out.  lev [M], last [N], order [M] and cnt [M + 2] are work space.
 __global__ void static_setup_kernel(const int32_t* rows, int M, int dmax, int N, int32_t* cols,
-                                    int32_t* runs, int32_t* n_runs, uint32_t* bitmap) {
+                                    int32_t* runs, int32_t* n_runs, uint32_t* bitmap, int32_t* lev,
+                                    int32_t* last, int32_t* order, int32_t* cnt) {
+    const unsigned full = 0xFFFFFFFFu;
     const int lane = threadIdx.x;
-    for (int i = lane; i < M * dmax; i += 32) cols[(i % dmax) * M + i / dmax] = rows[i];
+    for (int c = lane; c < N; c += 32) last[c] = 0;
     for (int w = lane; w < (N + 31) / 32; w += 32) bitmap[w] = 0u;
     __syncwarp();
-    int nr = 0, start = 0;
-    if (lane == 0) runs[0] = 0;
+    // earliest levels, rows in file order (a row's columns on its lanes)
+    int maxl = 0;
     for (int m = 0; m < M; ++m) {
         const int c = lane < dmax ? rows[(size_t)m * dmax + lane] : -1;
+        const int l = __reduce_max_sync(full, c >= 0 ? last[c] : 0) + 1;
+        __syncwarp();
+        if (c >= 0) last[c] = l;
+        if (lane == 0) lev[m] = l;
+        maxl = max(maxl, l);
+        __syncwarp();
+    }
+    // stable counting sort by level: cnt[l] = first position of level l
+    for (int l = lane; l < maxl + 2; l += 32) cnt[l] = 0;
+    __syncwarp();
+    for (int m = lane; m < M; m += 32) atomicAdd(&cnt[lev[m]], 1);
+    __syncwarp();
+    if (lane == 0) {
+        int s = 0;
+        for (int l = 1; l <= maxl; ++l) {
+            const int t = cnt[l];
+            cnt[l] = s;
+            s += t;
+        }
+    }
+    __syncwarp();
+    for (int m0 = 0; m0 < M; m0 += 32) {
+        const int m = m0 + lane;
+        const int l = m < M ? lev[m] : -1;
+        const unsigned peers = __match_any_sync(full, l);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int base = m < M ? cnt[l] : 0;
+        __syncwarp();
+        if (m < M) {
+            order[base + rank] = m;
+            if (lane == 31 - __clz(peers)) cnt[l] = base + __popc(peers);
+        }
+        __syncwarp();
+    }
+    // the table in schedule order
+    for (int i = lane; i < M * dmax; i += 32) cols[(i % dmax) * M + i / dmax] = rows[(size_t)order[i / dmax] * dmax + i % dmax];
+    __syncwarp();
+    // greedy steps of at most 32 rows sharing no variable
+    int nr = 0, start = 0;
+    if (lane == 0) runs[0] = 0;
+    for (int k = 0; k < M; ++k) {
+        const int c = lane < dmax ? rows[(size_t)order[k] * dmax + lane] : -1;
         const bool clash = c >= 0 && ((bitmap[c >> 5] >> (c & 31)) & 1u);
-        if (__any_sync(0xFFFFFFFFu, clash)) {
+        if (__any_sync(full, clash) || k - start == 32) {
             ++nr;
-            if (lane == 0) runs[nr] = m;
-            for (int r = start; r < m; ++r) {
-                const int c2 = lane < dmax ? rows[(size_t)r * dmax + lane] : -1;
+            if (lane == 0) runs[nr] = k;
+            for (int j = start; j < k; ++j) {
+                const int c2 = lane < dmax ? rows[(size_t)order[j] * dmax + lane] : -1;
                 if (c2 >= 0) atomicAnd(&bitmap[c2 >> 5], ~(1u << (c2 & 31)));
             }
-            start = m;
+            start = k;
             __syncwarp();
         }
         if (c >= 0) atomicOr(&bitmap[c >> 5], 1u << (c & 31));
@@ -482,7 +569,11 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     const size_t off_cols = off_rows + align256((size_t)M * dmax * 4);
     const size_t off_runs = off_cols + align256((size_t)M * dmax * 4);
     const size_t off_bits = off_runs + align256((size_t)(M + 2) * 4);
-    const size_t off_msgs = off_bits + align256((size_t)(N + 31) / 32 * 4);
+    const size_t off_lev = off_bits + align256((size_t)(N + 31) / 32 * 4);
+    const size_t off_last = off_lev + align256((size_t)M * 4);
+    const size_t off_order = off_last + align256((size_t)N * 4);
+    const size_t off_cnt = off_order + align256((size_t)M * 4);
+    const size_t off_msgs = off_cnt + align256((size_t)(M + 2) * 4);
     const size_t per_slot = (size_t)dmax * M * rsz;
     if (off_msgs + GEN_WARPS * per_slot > LDPC_STATIC_SCRATCH_BYTES) {
         snprintf(msg, sizeof msg,
@@ -539,7 +630,11 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_rows, h->rows, (size_t)M * dmax * 4, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
-        static_setup_kernel<<<1, 32, 0, stream>>>(d_rows, M, dmax, N, d_cols, d_runs, d_nruns, d_bits);
+        static_setup_kernel<<<1, 32, 0, stream>>>(d_rows, M, dmax, N, d_cols, d_runs, d_nruns, d_bits,
+                                                  reinterpret_cast<int32_t*>(base + off_lev),
+                                                  reinterpret_cast<int32_t*>(base + off_last),
+                                                  reinterpret_cast<int32_t*>(base + off_order),
+                                                  reinterpret_cast<int32_t*>(base + off_cnt));
         e = cudaGetLastError();
     }
     int32_t n_runs = 0;

@@ -248,6 +248,22 @@ extern "C" int ldpc_create(const ldpc_matrix* m, int device, ldpc_handle** out) 
     return 0;
 }
 
+extern "C" int ldpc_row_schedule(const ldpc_matrix* m, int32_t* order, int32_t* starts) {
+    if (!m || !m->rows || !order || !starts) return fail(LDPC_EINVAL, "matrix or output is NULL");
+    if (m->n_vars <= 0 || m->n_checks <= 0 || m->max_check_deg <= 0 || m->max_check_deg > 64)
+        return fail(LDPC_EINVAL, "bad matrix dimensions N=%d M=%d max_check_deg=%d", m->n_vars, m->n_checks,
+                    m->max_check_deg);
+    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i)
+        if (m->rows[i] >= m->n_vars || m->rows[i] < -1)
+            return fail(LDPC_EINVAL, "edge index out of bounds: row=%lld, col=%d",
+                        (long long)(i / m->max_check_deg) + 1, m->rows[i] + 1);
+    std::vector<int32_t> o, st;
+    general_schedule(m->rows, m->n_vars, m->n_checks, m->max_check_deg, o, st);
+    std::copy(o.begin(), o.end(), order);
+    std::copy(st.begin(), st.end(), starts);
+    return (int)st.size() - 1;
+}
+
 extern "C" int ldpc_kernel_kind(const ldpc_handle* h) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     return h->kind;

@@ -1,17 +1,19 @@
 // Decoder for an arbitrary parity-check matrix with the reference's serial row order.
 //
 // The reference updates rows one after another in file order (engines/scalar_5w/ldpc_decoder_core.h:
-// 314-522).  The host splits that order into runs of consecutive rows that share no variable; rows of
-// one run are independent, so updating them at once gives the serial result bit for bit.  One warp
-// owns one frame: lanes take the rows of a run (32 at a time), __syncwarp between runs.  L lives in
-// shared memory; the messages r of a slot live in a global-memory scratch area laid out [edge][row] so
-// a warp's accesses to one edge of 32 consecutive rows coalesce (the area of all resident slots,
-// E x 2-4 bytes each, stays in L2).
+// 314-522).  The host reorders the rows into steps of at most 32 rows that share no variable, keeping
+// every pair of rows that share one in file order (general_schedule in general.cu); rows of one step
+// are independent, so updating them at once gives the serial result bit for bit.  One warp owns one
+// frame: lanes take the rows of a step, __syncwarp between steps.  L lives in shared memory; the
+// messages r of a slot live in a global-memory scratch area laid out [edge][position in the schedule]
+// so a warp's accesses to one edge of a step coalesce (the area of all resident slots, E x 2-4 bytes
+// each, stays in L2).
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/ldpcb200.h"
 #include "ldpc_device.cuh"
@@ -22,8 +24,8 @@ constexpr int GEN_WARPS = 4;  // frame slots (warps) per CTA
 
 struct GeneralCode {
     int N = 0, M = 0, P = 0, dmax = 0, n_runs = 0, dt = 0;  // dt: compiled degree bound
-    int32_t* d_cols = nullptr;  // [dmax][M] column of edge e of row m (-1 pad)
-    int32_t* d_runs = nullptr;  // [n_runs + 1] first row of each run, then M
+    int32_t* d_cols = nullptr;  // [dmax][M] column of edge e of the row at schedule position k (-1 pad)
+    int32_t* d_runs = nullptr;  // [n_runs + 1] first position of each step, then M
     void* d_r = nullptr;        // message scratch: [slots][dmax][M] elements
     size_t r_cap = 0;
 };
@@ -50,6 +52,8 @@ struct GenParams {
     unsigned long long* snr_bins;
 };
 
+void general_schedule(const int32_t* rows, int N, int M, int dmax, std::vector<int32_t>& order,
+                      std::vector<int32_t>& starts);
 int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCode* g, std::string& err);
 void free_general(GeneralCode* g);
 // No-allocation variant of ldpc_decode_llr (device buffers, static scratch); see general.cu.

@@ -29,7 +29,8 @@ EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", 
            "ldpc_set_circulant",
            "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
-           "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_last_error", "ldpc_abi_version")
+           "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_row_schedule", "ldpc_last_error",
+           "ldpc_abi_version")
 
 
 class LdpcError(RuntimeError):
@@ -123,6 +124,7 @@ def load(path: str = LIB_PATH):
     L.ldpc_launch_param_bytes.restype = C.c_int64
     L.ldpc_decode_llr_static.argtypes = [P(Matrix), P(RunParams), C.c_void_p, C.c_int64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p, P(Tally), C.c_void_p]
+    L.ldpc_row_schedule.argtypes = [P(Matrix), P(C.c_int32), P(C.c_int32)]
     L.ldpc_last_error.argtypes = [C.c_char_p, C.c_size_t]
     L.ldpc_abi_version.argtypes = []
     _lib = L
@@ -175,6 +177,20 @@ def decode_llr_static(rows: np.ndarray, n_vars: int, n_punct: int, p: RunParams,
                                       stream or None))
     return ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
                        t.kernel_ms, t.bit_errors_sq)
+
+
+def row_schedule(rows: np.ndarray, n_vars: int):
+    """ldpc_row_schedule (host only, no GPU): the general kernel's row schedule of a [M, dmax] row
+    table.  Returns (order, starts): the file rows in schedule order and the first position of every
+    step followed by M."""
+    lib = load()
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    M = rows.shape[0]
+    m = Matrix(int(n_vars), M, 0, rows.shape[1], _ip(rows))
+    order = np.zeros(M, np.int32)
+    starts = np.zeros(M + 1, np.int32)
+    n = _check(lib.ldpc_row_schedule(C.byref(m), _ip(order), _ip(starts)))
+    return order, starts[:n + 1].copy()
 
 
 @dataclass

@@ -152,6 +152,39 @@ def match_ar4ja(mat: Matrix) -> Optional[ar4ja.QcCode]:
     return None
 
 
+def row_schedule(mat: Matrix):
+    """The general kernel's row schedule (the library's ldpc_row_schedule, restated).
+
+    Rows that share no variable commute bit for bit, so any order that keeps every pair of rows
+    sharing a variable in file order decodes as the file order does.  Each row's earliest level is
+    1 + the highest level among the earlier rows it shares a variable with; the rows sorted by level
+    (file order inside a level) are cut greedily into steps of consecutive rows that share no
+    variable, at most 32 rows each.  Returns (order, starts): the file rows in schedule order and the
+    first position of every step followed by M.
+    """
+    last = {}
+    lev = []
+    for r in mat.rows:
+        cols = [int(v) for v in r if v >= 0]
+        lv = 1 + max((last.get(c, 0) for c in cols), default=0)
+        lev.append(lv)
+        for c in cols:
+            last[c] = lv
+    order = sorted(range(mat.M), key=lambda m: (lev[m], m))
+    starts = [0]
+    used = set()
+    start = 0
+    for k, m in enumerate(order):
+        s = set(int(v) for v in mat.rows[m] if v >= 0)
+        if k - start == 32 or (used & s):
+            starts.append(k)
+            used = set()
+            start = k
+        used |= s
+    starts.append(mat.M)
+    return order, starts
+
+
 def conflict_free_runs(mat: Matrix) -> List[int]:
     """Greedy split of the serial row order into runs of consecutive rows that share no variable.
 
