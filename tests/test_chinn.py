@@ -66,3 +66,21 @@ def test_conflict_free_runs_makeh_order():
     m = chinn.Matrix(N=c.N, M=c.n_checks, max_var_deg=6, max_check_deg=6, rows=c.rows())
     runs = chinn.conflict_free_runs(m)
     assert runs == [i * 128 for i in range(13)]  # exactly the 12 layers of Z = 128 rows
+
+
+def test_chinn_out_text_round_trip(tmp_path):
+    """A row table written as .chinn.out reads back with the same rows in the same edge order (the
+    shipped matrix rebuilt from the committed fixture)."""
+    import numpy as np
+    import conftest
+    g = np.load(conftest.GOLDEN)
+    rows = g["shipped_rows"].astype(np.int32)
+    p = tmp_path / "shipped.chinn.out"
+    p.write_text(chinn.chinn_out_text(rows, 2560))
+    m = chinn.parse_chinn(str(p))
+    assert (m.M, m.N) == rows.shape[:1] + (2560,)
+    for r, back in zip(rows, m.rows):
+        assert back.tolist() == r[r >= 0].tolist()
+    rr = np.array([[2, 0, -1], [1, -1, -1]], np.int32)  # an edge order that is not ascending
+    p.write_text(chinn.chinn_out_text(rr, 3))
+    assert [r.tolist() for r in chinn.parse_chinn(str(p)).rows] == [[2, 0], [1]]

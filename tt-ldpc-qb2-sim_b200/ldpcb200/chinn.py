@@ -93,6 +93,18 @@ def parse_chinn_out(path: str) -> Matrix:
                   rows=[np.array(r, dtype=np.int32) for r in rows], path=path)
 
 
+def chinn_out_text(rows, N: int) -> str:
+    """A row table ([M, dmax] with -1 after each row's last edge, or a list of per-row arrays) as a
+    ``.chinn.out`` file that ``parse_chinn_out`` reads back with the same rows in the same edge
+    order: 1-based ``row col 1.000000`` triplets, row by row and each row's edges in order, closed by
+    ``M N 0.000000``."""
+    lines = []
+    for m, r in enumerate(rows):
+        lines.extend(f"{m + 1}\t{int(c) + 1}\t1.000000 " for c in r if c >= 0)
+    lines.append(f"{len(rows)}\t{N}\t0.000000 ")
+    return "\n".join(lines) + "\n"
+
+
 def parse_chinn(path: str) -> Matrix:
     """``ldpc_sim_scalar.cpp:204-269``: auto-detects the triplet format."""
     if not os.path.exists(path):
