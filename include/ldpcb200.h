@@ -54,7 +54,8 @@ typedef struct ldpc_handle ldpc_handle;
 
 /* A parity-check matrix: replaces the reference's ChinnMatrix (ldpc_sim_scalar.cpp:108-114).
  * rows[m * max_check_deg + d] is the 0-based column of edge d of check m, in the order the matrix
- * file lists it, -1 after the row's last edge.  The last n_punct columns are punctured. */
+ * file lists it, -1 after the row's last edge (an edge after a -1 is rejected with LDPC_EINVAL).  The
+ * last n_punct columns are punctured. */
 typedef struct {
     int32_t n_vars;        /* N */
     int32_t n_checks;      /* M (checks) */

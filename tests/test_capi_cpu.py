@@ -57,6 +57,14 @@ def test_bad_arguments_are_rejected_before_any_device_work():
     assert "out of bounds" in capi.last_error()
     m = capi.Matrix(3, 1, 3, 2, rows.ctypes.data_as(C.POINTER(C.c_int32)))
     assert lib.ldpc_create(C.byref(m), 0, C.byref(h)) == -22
+    holed = np.array([[0, -1, 2]], np.int32)  # an edge after the -1 that ends the row
+    m = capi.Matrix(3, 1, 0, 3, holed.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert lib.ldpc_create(C.byref(m), 0, C.byref(h)) == -22
+    assert "ends the row" in capi.last_error()
+    with pytest.raises(capi.LdpcError):
+        capi.row_schedule(holed, 3)
+    with pytest.raises(capi.LdpcError):
+        capi.decode_llr_static(holed, 3, 0, capi.RunParams(), 0, 0)
     t = capi.Tally()
     assert lib.ldpc_run_chunk(None, None, C.byref(t)) == -22
     assert lib.ldpc_set_circulant(None, C.byref(capi.CircConfig(1, 1, 0.9375, 0))) == -22

@@ -10,27 +10,62 @@
 
 namespace ldpcb200 {
 
+// Row-major tables of the general kernel, each row padded to a multiple of 16 bytes so that one
+// lane reads a row's columns and messages with 16-byte loads: columns [M][gen_dtc(DT)] int32 (-1
+// after the row's last edge), messages [M][gen_dtr<MODE>(DT)] elements per frame slot.
+__host__ __device__ constexpr int gen_dtc(int dt) { return (dt + 3) & ~3; }
+template <int MODE>
+__host__ __device__ constexpr int gen_dtr(int dt) {
+    return MODE == STORE_FP32 ? (dt + 3) & ~3 : (dt + 7) & ~7;
+}
+
+// Message bytes of one frame slot.
+static size_t gen_slot_bytes(int M, int dt, int storage) {
+    return storage == STORE_FP32 ? (size_t)M * gen_dtr<STORE_FP32>(dt) * 4 : (size_t)M * gen_dtr<STORE_BF16>(dt) * 2;
+}
+
+template <int DT>
+__device__ __forceinline__ void gen_load_cols(const int32_t* cols, int m, int (&col)[gen_dtc(DT)]) {
+    const int4* cp = reinterpret_cast<const int4*>(cols + (size_t)m * gen_dtc(DT));
+#pragma unroll
+    for (int k = 0; k < gen_dtc(DT) / 4; ++k) {
+        const int4 v = __ldg(cp + k);
+        col[4 * k] = v.x;
+        col[4 * k + 1] = v.y;
+        col[4 * k + 2] = v.z;
+        col[4 * k + 3] = v.w;
+    }
+}
+
 // One row of degree deg <= DT, updated by one lane (ldpc_decoder_core.h:414-520).
 template <int DT, int MODE, int ALGO>
 __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTraits<MODE>::T* L,
                                         typename RTraits<MODE>::T* r, float r_cap, float lp_cap) {
     using LT = LTraits<MODE>;
     using RT = RTraits<MODE>;
-    const int M = p.M;
+    using RE = typename RT::T;
+    constexpr int DTR = gen_dtr<MODE>(DT);
+    constexpr int NV = DTR * (int)sizeof(RE) / 16;
     int deg = 0;
-    int col[DT];
+    int col[gen_dtc(DT)];
     float q[DT];
+    gen_load_cols<DT>(p.cols, m, col);
 #pragma unroll
-    for (int e = 0; e < DT; ++e) {
-        col[e] = e < p.dmax ? p.cols[e * M + m] : -1;
+    for (int e = 0; e < DT; ++e)
         if (col[e] >= 0) deg = e + 1;
-    }
     if (deg == 0) return;
+    union {
+        uint4 v[NV];
+        RE e[DTR];
+    } rm;
+    uint4* rp = reinterpret_cast<uint4*>(r + (size_t)m * DTR);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) rm.v[k] = rp[k];
     uint32_t par = 0;
 #pragma unroll
     for (int e = 0; e < DT; ++e)
         if (e < deg) {
-            q[e] = __fsub_rn(LT::ld(L, col[e]), RT::ld(r + (size_t)e * M + m));
+            q[e] = __fsub_rn(LT::ld(L, col[e]), RT::ld(&rm.e[e]));
             par ^= __float_as_uint(q[e]);
         }
     par &= 0x80000000u;
@@ -85,8 +120,10 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
             float ln = __fadd_rn(q[e], rn);
             ln = fminf(fmaxf(ln, -lp_cap), lp_cap);
             LT::st(L, col[e], ln);
-            RT::st(r + (size_t)e * M + m, rn);
+            RT::st(&rm.e[e], rn);
         }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) rp[k] = rm.v[k];
 }
 
 // NW: frame slots (warps) per CTA; large codes use one so that a slot's L fits shared memory.
@@ -101,7 +138,7 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
     const int lstride = (N + 7) & ~7;
     LE* L = reinterpret_cast<LE*>(smem_raw) + (size_t)warp * lstride;
     const size_t slot = (size_t)blockIdx.x * NW + warp;
-    RE* r = reinterpret_cast<RE*>(p.r_base) + slot * (size_t)p.dmax * M;
+    RE* r = reinterpret_cast<RE*>(p.r_base) + slot * (size_t)M * gen_dtr<MODE>(DT);
     const float r_cap = p.r_max > 0.0f ? p.r_max : __int_as_float(0x7f800000);
     const float lp_cap = p.l_post_max > 0.0f ? p.l_post_max : __int_as_float(0x7f800000);
     unsigned long long t_frames = 0, t_be = 0, t_fe = 0, t_it = 0, t_unc = 0, t_max = 0, t_be2 = 0;
@@ -144,7 +181,11 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
             }
         }
         for (int i = p.n_tx + lane; i < N; i += 32) LT::st(L, i, 0.0f);
-        for (size_t i = lane; i < (size_t)p.dmax * M; i += 32) r[i] = RE(0);
+        {
+            uint4* rz = reinterpret_cast<uint4*>(r);
+            const size_t nv = (size_t)M * gen_dtr<MODE>(DT) * sizeof(RE) / 16;
+            for (size_t i = lane; i < nv; i += 32) rz[i] = make_uint4(0u, 0u, 0u, 0u);
+        }
         __syncwarp();
 
         int it = 0;
@@ -164,12 +205,13 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
                 for (int m0 = 0; m0 < M && !bad; m0 += 32) {
                     const int m = m0 + lane;
                     uint32_t par = 0;
-                    if (m < M)
-                        for (int e = 0; e < p.dmax; ++e) {
-                            const int c = p.cols[e * M + m];
-                            if (c < 0) break;
-                            par ^= __float_as_uint(LT::ld(L, c)) >> 31;
-                        }
+                    if (m < M) {
+                        int col[gen_dtc(DT)];
+                        gen_load_cols<DT>(p.cols, m, col);
+#pragma unroll
+                        for (int e = 0; e < DT; ++e)
+                            if (col[e] >= 0) par ^= __float_as_uint(LT::ld(L, col[e])) >> 31;
+                    }
                     bad = __any_sync(0xFFFFFFFFu, par) != 0;
                 }
                 if (!bad) break;
@@ -181,11 +223,11 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
         be = __reduce_add_sync(0xFFFFFFFFu, be);
         for (int m = lane; m < M; m += 32) {
             uint32_t par = 0;
-            for (int e = 0; e < p.dmax; ++e) {
-                const int c = p.cols[e * M + m];
-                if (c < 0) break;
-                par ^= __float_as_uint(LT::ld(L, c)) >> 31;
-            }
+            int col[gen_dtc(DT)];
+            gen_load_cols<DT>(p.cols, m, col);
+#pragma unroll
+            for (int e = 0; e < DT; ++e)
+                if (col[e] >= 0) par ^= __float_as_uint(LT::ld(L, col[e])) >> 31;
             sfail += par;
         }
         sfail = __reduce_add_sync(0xFFFFFFFFu, sfail);
@@ -293,19 +335,21 @@ int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCod
     g->P = P;
     g->dmax = dmax;
     int maxdeg = 0;
+    for (int m = 0; m < M; ++m)
+        for (int e = 0; e < dmax && rows[(size_t)m * dmax + e] >= 0; ++e) maxdeg = std::max(maxdeg, e + 1);
+    g->dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : maxdeg <= 32 ? 32 : 0;
+    if (!g->dt) return gfail(err, LDPC_ENOTSUP, "row degree above 32 is not supported");
     std::vector<int32_t> order, runs;
     general_schedule(rows, N, M, dmax, order, runs);
-    std::vector<int32_t> cols((size_t)dmax * M, -1);
+    g->n_runs = (int)runs.size() - 1;
+    const int dtc = gen_dtc(g->dt);
+    std::vector<int32_t> cols((size_t)dtc * M, -1);  // [M][dtc], rows in schedule order
     for (int k = 0; k < M; ++k)
         for (int e = 0; e < dmax; ++e) {
             const int32_t c = rows[(size_t)order[k] * dmax + e];
             if (c < 0) break;
-            cols[(size_t)e * M + k] = c;
-            maxdeg = std::max(maxdeg, e + 1);
+            cols[(size_t)k * dtc + e] = c;
         }
-    g->n_runs = (int)runs.size() - 1;
-    g->dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : maxdeg <= 32 ? 32 : 0;
-    if (!g->dt) return gfail(err, LDPC_ENOTSUP, "row degree above 32 is not supported");
     if (cudaMalloc(&g->d_cols, cols.size() * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&g->d_runs, runs.size() * sizeof(int32_t)) != cudaSuccess) {
         cudaGetLastError();
@@ -373,8 +417,7 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
     const uint64_t want = (n + nw - 1) / nw;
     const uint64_t grid = std::min<uint64_t>(want, (uint64_t)per_sm * n_sm);
     if (!grid) return 0;
-    const size_t rsz = p->storage == STORE_FP32 ? 4 : 2;
-    const size_t need = grid * nw * (size_t)g->dmax * g->M * rsz;
+    const size_t need = grid * nw * gen_slot_bytes(g->M, g->dt, p->storage);
     if (g->r_cap < need) {
         cudaFree(g->d_r);
         g->d_r = nullptr;
@@ -438,7 +481,7 @@ int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t 
 // Scratch layout (LDPC_STATIC_SCRATCH_BYTES, 256-byte aligned regions):
 //   [0, 256)           frame-claim counter (u32) and tallies (TALLY_WORDS x u64)
 //   rows               the caller's [M][dmax] row table, copied in
-//   cols               the same table transposed to [dmax][M] (the general kernel's layout)
+//   cols               the same table in schedule order, [M][dtc] (the general kernel's layout)
 //   runs               step starts (M + 1 entries) and their count
 //   bitmap             N bits, used while the steps are cut
 //   lev, last, order, cnt   work space of the schedule: M, N, M and M + 2 ints
@@ -458,9 +501,9 @@ unsigned char* g_static_addr[kMaxDevices] = {};
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // The schedule of general_schedule on the device (the same levels, order and steps), one warp, no
-// waits on other threads: the caller's [M][dmax] row table in, the [dmax][M] table in schedule order
+// waits on other threads: the caller's [M][dmax] row table in, the [M][dtc] table in schedule order
 // and the step starts out.  lev [M], last [N], order [M] and cnt [M + 2] are work space.
-__global__ void static_setup_kernel(const int32_t* rows, int M, int dmax, int N, int32_t* cols,
+__global__ void static_setup_kernel(const int32_t* rows, int M, int dmax, int N, int dtc, int32_t* cols,
                                     int32_t* runs, int32_t* n_runs, uint32_t* bitmap, int32_t* lev,
                                     int32_t* last, int32_t* order, int32_t* cnt) {
     const unsigned full = 0xFFFFFFFFu;
@@ -506,8 +549,11 @@ __global__ void static_setup_kernel(const int32_t* rows, int M, int dmax, int N,
         }
         __syncwarp();
     }
-    // the table in schedule order
-    for (int i = lane; i < M * dmax; i += 32) cols[(i % dmax) * M + i / dmax] = rows[(size_t)order[i / dmax] * dmax + i % dmax];
+    // the table in schedule order, [M][dtc]
+    for (int i = lane; i < M * dtc; i += 32) {
+        const int k = i / dtc, e = i % dtc;
+        cols[i] = e < dmax ? rows[(size_t)order[k] * dmax + e] : -1;
+    }
     __syncwarp();
     // greedy steps of at most 32 rows sharing no variable
     int nr = 0, start = 0;
@@ -560,21 +606,23 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     for (int64_t i = 0; i < (int64_t)M * dmax; ++i) {
         const int32_t c = h->rows[i];
         if (c < -1 || c >= N) return sfail(LDPC_EINVAL, err, "edge index out of bounds");
+        if (c >= 0 && i % dmax > 0 && h->rows[i - 1] < 0)
+            return sfail(LDPC_EINVAL, err, "edge after the -1 that ends its row");
         if (c >= 0) maxdeg = std::max(maxdeg, (int)(i % dmax) + 1);
     }
     const int dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : 32;
+    const int dtc = gen_dtc(dt);
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
-    const size_t rsz = p->storage == STORE_FP32 ? 4 : 2;
     const size_t off_rows = 256;
     const size_t off_cols = off_rows + align256((size_t)M * dmax * 4);
-    const size_t off_runs = off_cols + align256((size_t)M * dmax * 4);
+    const size_t off_runs = off_cols + align256((size_t)M * dtc * 4);
     const size_t off_bits = off_runs + align256((size_t)(M + 2) * 4);
     const size_t off_lev = off_bits + align256((size_t)(N + 31) / 32 * 4);
     const size_t off_last = off_lev + align256((size_t)M * 4);
     const size_t off_order = off_last + align256((size_t)N * 4);
     const size_t off_cnt = off_order + align256((size_t)M * 4);
     const size_t off_msgs = off_cnt + align256((size_t)(M + 2) * 4);
-    const size_t per_slot = (size_t)dmax * M * rsz;
+    const size_t per_slot = gen_slot_bytes(M, dt, p->storage);
     if (off_msgs + GEN_WARPS * per_slot > LDPC_STATIC_SCRATCH_BYTES) {
         snprintf(msg, sizeof msg,
                  "matrix needs %zu bytes of static scratch for one CTA of %d frame slots; the maximum is %zu",
@@ -630,7 +678,7 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_rows, h->rows, (size_t)M * dmax * 4, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
-        static_setup_kernel<<<1, 32, 0, stream>>>(d_rows, M, dmax, N, d_cols, d_runs, d_nruns, d_bits,
+        static_setup_kernel<<<1, 32, 0, stream>>>(d_rows, M, dmax, N, dtc, d_cols, d_runs, d_nruns, d_bits,
                                                   reinterpret_cast<int32_t*>(base + off_lev),
                                                   reinterpret_cast<int32_t*>(base + off_last),
                                                   reinterpret_cast<int32_t*>(base + off_order),

@@ -200,10 +200,14 @@ extern "C" int ldpc_create(const ldpc_matrix* m, int device, ldpc_handle** out) 
                     m->n_checks, m->max_check_deg);
     if (m->n_punct < 0 || m->n_punct >= m->n_vars)
         return fail(LDPC_EINVAL, "punctured count %d outside [0, N)", m->n_punct);
-    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i)
+    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i) {
         if (m->rows[i] >= m->n_vars || m->rows[i] < -1)
             return fail(LDPC_EINVAL, "edge index out of bounds: row=%lld, col=%d",
                         (long long)(i / m->max_check_deg) + 1, m->rows[i] + 1);
+        if (m->rows[i] >= 0 && i % m->max_check_deg > 0 && m->rows[i - 1] < 0)
+            return fail(LDPC_EINVAL, "row %lld: edge after the -1 that ends the row",
+                        (long long)(i / m->max_check_deg) + 1);
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -253,10 +257,14 @@ extern "C" int ldpc_row_schedule(const ldpc_matrix* m, int32_t* order, int32_t* 
     if (m->n_vars <= 0 || m->n_checks <= 0 || m->max_check_deg <= 0 || m->max_check_deg > 64)
         return fail(LDPC_EINVAL, "bad matrix dimensions N=%d M=%d max_check_deg=%d", m->n_vars, m->n_checks,
                     m->max_check_deg);
-    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i)
+    for (int64_t i = 0; i < (int64_t)m->n_checks * m->max_check_deg; ++i) {
         if (m->rows[i] >= m->n_vars || m->rows[i] < -1)
             return fail(LDPC_EINVAL, "edge index out of bounds: row=%lld, col=%d",
                         (long long)(i / m->max_check_deg) + 1, m->rows[i] + 1);
+        if (m->rows[i] >= 0 && i % m->max_check_deg > 0 && m->rows[i - 1] < 0)
+            return fail(LDPC_EINVAL, "row %lld: edge after the -1 that ends the row",
+                        (long long)(i / m->max_check_deg) + 1);
+    }
     std::vector<int32_t> o, st;
     general_schedule(m->rows, m->n_vars, m->n_checks, m->max_check_deg, o, st);
     std::copy(o.begin(), o.end(), order);

@@ -5,9 +5,9 @@
 // every pair of rows that share one in file order (general_schedule in general.cu); rows of one step
 // are independent, so updating them at once gives the serial result bit for bit.  One warp owns one
 // frame: lanes take the rows of a step, __syncwarp between steps.  L lives in shared memory; the
-// messages r of a slot live in a global-memory scratch area laid out [edge][position in the schedule]
-// so a warp's accesses to one edge of a step coalesce (the area of all resident slots, E x 2-4 bytes
-// each, stays in L2).
+// messages r of a slot live in a global-memory scratch area laid out [position in the schedule][edge],
+// each row padded to a multiple of 16 bytes, so a lane reads and writes its row's messages with
+// 16-byte accesses and a step's rows are contiguous (the area of all resident slots stays in L2).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -24,9 +24,9 @@ constexpr int GEN_WARPS = 4;  // frame slots (warps) per CTA
 
 struct GeneralCode {
     int N = 0, M = 0, P = 0, dmax = 0, n_runs = 0, dt = 0;  // dt: compiled degree bound
-    int32_t* d_cols = nullptr;  // [dmax][M] column of edge e of the row at schedule position k (-1 pad)
+    int32_t* d_cols = nullptr;  // [M][gen_dtc(dt)] columns of the row at schedule position k (-1 pad)
     int32_t* d_runs = nullptr;  // [n_runs + 1] first position of each step, then M
-    void* d_r = nullptr;        // message scratch: [slots][dmax][M] elements
+    void* d_r = nullptr;        // message scratch: [slots][M][gen_dtr(dt)] elements
     size_t r_cap = 0;
 };
 
