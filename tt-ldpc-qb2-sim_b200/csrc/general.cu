@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "ldpc_general.cuh"
@@ -10,13 +11,17 @@
 
 namespace ldpcb200 {
 
-// Row-major tables of the general kernel, each row padded to a multiple of 16 bytes so that one
-// lane reads a row's columns and messages with 16-byte loads: columns [M][gen_dtc(DT)] int32 (-1
-// after the row's last edge), messages [M][gen_dtr<MODE>(DT)] elements per frame slot.
+// Row-major tables of the general kernel, so that one lane reads a row's columns and messages with
+// a few vector loads: columns [M][gen_dtc(DT)] int32 (-1 after the row's last edge), each row padded
+// to a multiple of 4 (16 bytes); messages [M][gen_dtr<MODE>(DT)] elements per frame slot, rows
+// unpadded (16-bit rows rounded to an even count), read and written with the widest vectors that
+// tile a row (16, 8 or 4 bytes: 4 for 12-byte bf16 rows of degree 6, 8 for 24-byte fp32 ones).
+// Padding the messages to 16 bytes as well was slower (bf16 9.93 vs 10.18, fp32 6.91 vs 8.25 M
+// frames/s on the shipped r1/2 K=1024 file): the scratch of all resident slots outgrew L2.
 __host__ __device__ constexpr int gen_dtc(int dt) { return (dt + 3) & ~3; }
 template <int MODE>
 __host__ __device__ constexpr int gen_dtr(int dt) {
-    return MODE == STORE_FP32 ? (dt + 3) & ~3 : (dt + 7) & ~7;
+    return MODE == STORE_FP32 ? dt : (dt + 1) & ~1;
 }
 
 // Message bytes of one frame slot.
@@ -45,7 +50,11 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
     using RT = RTraits<MODE>;
     using RE = typename RT::T;
     constexpr int DTR = gen_dtr<MODE>(DT);
-    constexpr int NV = DTR * (int)sizeof(RE) / 16;
+    constexpr int RB = DTR * (int)sizeof(RE);
+    constexpr int VW = RB % 16 == 0 ? 16 : RB % 8 == 0 ? 8 : 4;
+    constexpr int NV = RB / VW;
+    using VT = typename std::conditional<VW == 16, uint4,
+                                         typename std::conditional<VW == 8, uint2, uint32_t>::type>::type;
     int deg = 0;
     int col[gen_dtc(DT)];
     float q[DT];
@@ -55,10 +64,10 @@ __device__ __forceinline__ void gen_row(const GenParams& p, int m, typename LTra
         if (col[e] >= 0) deg = e + 1;
     if (deg == 0) return;
     union {
-        uint4 v[NV];
+        VT v[NV];
         RE e[DTR];
     } rm;
-    uint4* rp = reinterpret_cast<uint4*>(r + (size_t)m * DTR);
+    VT* rp = reinterpret_cast<VT*>(r + (size_t)m * DTR);
 #pragma unroll
     for (int k = 0; k < NV; ++k) rm.v[k] = rp[k];
     uint32_t par = 0;
@@ -182,9 +191,9 @@ __global__ void __launch_bounds__(32 * NW) general_kernel(const __grid_constant_
         }
         for (int i = p.n_tx + lane; i < N; i += 32) LT::st(L, i, 0.0f);
         {
-            uint4* rz = reinterpret_cast<uint4*>(r);
-            const size_t nv = (size_t)M * gen_dtr<MODE>(DT) * sizeof(RE) / 16;
-            for (size_t i = lane; i < nv; i += 32) rz[i] = make_uint4(0u, 0u, 0u, 0u);
+            uint32_t* rz = reinterpret_cast<uint32_t*>(r);
+            const size_t nw = (size_t)M * gen_dtr<MODE>(DT) * sizeof(RE) / 4;
+            for (size_t i = lane; i < nw; i += 32) rz[i] = 0u;
         }
         __syncwarp();
 

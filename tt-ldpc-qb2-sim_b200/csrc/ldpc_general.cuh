@@ -6,8 +6,8 @@
 // are independent, so updating them at once gives the serial result bit for bit.  One warp owns one
 // frame: lanes take the rows of a step, __syncwarp between steps.  L lives in shared memory; the
 // messages r of a slot live in a global-memory scratch area laid out [position in the schedule][edge],
-// each row padded to a multiple of 16 bytes, so a lane reads and writes its row's messages with
-// 16-byte accesses and a step's rows are contiguous (the area of all resident slots stays in L2).
+// so a lane reads and writes its row's messages with a few vector accesses and a step's rows are
+// contiguous (the area of all resident slots stays mostly in L2).
 #pragma once
 #include <cuda_runtime.h>
 
