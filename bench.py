@@ -21,6 +21,12 @@ host thread on the same workload.
 threshold + 2.0] dB of each code, every code's persistent kernel a node of one CUDA graph, storage
 and launch shape autotuned per code (ldpcb200.mixed).
 
+``--workload file --matrix PATH [--punctured P]`` benchmarks any matrix file the drop-in engine
+binary accepts (``ldpc_sim -c PATH -p P``), e.g. the reference's shipped permuted r1/2 K=1024 file:
+the library picks the QC kernel for a matrix in makeH order and otherwise the general kernel (the
+file's serial row order, bit-exact), bf16 storage unless ``--storage`` says otherwise; its CPU
+baseline and reference arm run the reference's decoder on the same matrix.
+
 ``--workload circulant`` benchmarks the circulant engine's decoder (LDPC_ALGO_CIRC with the engine's
 silicon settings: SFPU arithmetic, damping 15/16, info-bit stop, bf16 storage) on the same code and
 points; its CPU baseline is the reference's golden stepper Monte Carlo
@@ -65,7 +71,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("error-floor", "mixed", "circulant"), default="error-floor")
+    ap.add_argument("--workload", choices=("error-floor", "mixed", "circulant", "file"), default="error-floor")
+    ap.add_argument("--matrix", default="", help="file workload: a .chinn / .chinn.out matrix")
+    ap.add_argument("--punctured", type=int, default=0, help="file workload: punctured columns (ldpc_sim -p)")
     ap.add_argument("--mixed-frames", type=int, default=1 << 24, help="mixed workload: frames per step per GPU")
     ap.add_argument("--frames", type=int, default=1 << 22, help="frames per Eb/N0 point per GPU per step")
     ap.add_argument("--storage", choices=("auto", "fp32", "fp16", "bf16"), default="auto",
@@ -84,6 +92,29 @@ def parse_args():
 def code_and_matrix():
     from ldpcb200 import ar4ja
     return ar4ja.make_code(1024, "1/2")
+
+
+class FileCode:
+    """A matrix file as the drop-in engine binary reads it (ldpcb200.chinn.parse_chinn)."""
+
+    def __init__(self, path: str, punctured: int):
+        from ldpcb200 import chinn
+        self.mat = chinn.parse_chinn(path)
+        self.name = os.path.basename(path)
+        self.N, self.n_checks, self.P = self.mat.N, self.mat.M, int(punctured)
+        if not 0 <= self.P < self.N:
+            raise SystemExit(f"--punctured {self.P} outside [0, N={self.N})")
+        self.n_tx = self.N - self.P
+        self.n_edges = int(sum(len(r) for r in self.mat.rows))
+
+    def row_matrix(self):
+        return self.mat.row_matrix()
+
+
+def file_code(args):
+    if not args.matrix:
+        raise SystemExit("--workload file needs --matrix PATH")
+    return FileCode(args.matrix, args.punctured)
 
 
 def mu_sigma(code, ebn0):
@@ -152,10 +183,10 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU baseline
-def cpu_baseline(seconds: float, threads: int = 0):
+def cpu_baseline(seconds: float, threads: int = 0, code=None):
     """The reference's own decoder (oracle/_ref/ref_mc) on every host thread, else the oracle port."""
     from oracle import oracle as O
-    code = code_and_matrix()
+    code = code or code_and_matrix()
     oc = O.Code(code.row_matrix(), code.N, code.P)
     threads = threads or os.cpu_count() or 1
     per_point = max(1.0, seconds / len(POINTS))
@@ -214,7 +245,7 @@ def run_reference(args):
     if args.workload == "circulant":
         return run_reference_circulant(args)
     from oracle import oracle as O
-    code = code_and_matrix()
+    code = file_code(args) if args.workload == "file" else code_and_matrix()
     oc = O.Code(code.row_matrix(), code.N, code.P)
     threads = os.cpu_count() or 1
     kind = "reference" if O.ref_binary("ref_mc") else "port"
@@ -238,7 +269,9 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: all-zero codeword, BPSK over AWGN, the reference's xoshiro128+/polar channel",
         "impl": "reference",
-        "config": {"workload": "AR4JA r1/2 K=1024 N=2560, Eb/N0 2.5 and 3.0 dB, max 200 iterations, syndrome stop",
+        "config": {"workload": (f"matrix {code.name} (N={code.N}, M={code.n_checks}, P={code.P})"
+                                if args.workload == "file" else "AR4JA r1/2 K=1024 N=2560") +
+                               ", Eb/N0 2.5 and 3.0 dB, max 200 iterations, syndrome stop",
                    "engine": "run_ldpc_worker (engines/scalar_5w/ldpc_decoder_core.h) on host threads",
                    "frames_per_s": round(frames / el, 1) if el > 0 else 0.0, "fer": fe / max(frames, 1)},
         "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": kind,
@@ -499,6 +532,125 @@ def run_ours(args):
                      "bytes_per_edge": BYTES_PER_EDGE[args.storage]},
             "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
             "hbm_peak_source": "measured (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "fallback (6.65 TB/s)",
+        },
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    dec.close()
+    return 0
+
+
+def run_file(args):
+    """Any matrix file on one GPU (or independent replicas with disjoint frames): the drop-in engine's
+    decode path for that file, timed like the error-floor line."""
+    import torch
+
+    from ldpcb200 import capi
+    from ldpcb200.dist import frame_range
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    code = file_code(args)
+    dec = capi.Decoder(code.row_matrix(), code.N, code.P, local)
+    kind = "qc" if dec.kind == capi.KERNEL_QC else "general"
+    storage = "bf16" if args.storage == "auto" else args.storage
+    F = args.frames
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step(i, acc=None):
+        for pi, eb in enumerate(POINTS):
+            mu, sigma = mu_sigma(code, eb)
+            first, _ = frame_range(i, world, rank, F)
+            p = dec.params(mu=mu, sigma=sigma, seed=SEED, stream=pi, first_frame=first, n_frames=F,
+                           max_iter=MAX_ITER, storage=storage)
+            t0 = time.perf_counter()
+            r = dec.run_chunk(p)
+            t1 = time.perf_counter()
+            if acc is not None:
+                a = acc[eb]
+                a["frames"] += r.frames; a["fe"] += r.frame_errors; a["be"] += r.bit_errors
+                a["iters"] += r.iter_sum; a["kernel_ms"] += r.kernel_ms; a["e2e_s"] += t1 - t0
+        flush.zero_()
+
+    for i in range(args.warmup):
+        step(10_000 + i)
+    acc = {eb: dict(frames=0, fe=0, be=0, iters=0, kernel_ms=0.0, e2e_s=0.0) for eb in POINTS}
+    launches0 = dec.launches
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(list(range(world)) if rank == 0 else []) as clk:
+        for i in range(args.steps):
+            step(i, acc)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+    launches = dec.launches - launches0
+    dev_s = sum(a["kernel_ms"] for a in acc.values()) / 1e3
+    e2e_s = sum(a["e2e_s"] for a in acc.values())
+    frames = sum(a["frames"] for a in acc.values())
+    iters = sum(a["iters"] for a in acc.values())
+    t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device="cuda")
+    n = torch.tensor([frames, iters, launches], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    dev_max, e2e_max = t.tolist()
+    tot_frames, _, tot_launches = n.tolist()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(args.cpu_seconds, code=code)
+        except Exception as e:
+            log(f"cpu baseline failed: {e}")
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        dec.close()
+        return 0
+    clocks = clk.summary()
+    f_mhz = clocks["sm_mhz"] if clocks else measured_peaks().get("sm_max_mhz", 1965.0)
+    ops = LANE_OPS_PER_EDGE * code.n_edges * iters
+    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
+    line = {
+        "metric": METRIC, "value": round(tot_frames * code.n_tx / dev_max / 1e9, 4), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * dev_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: all-zero codeword, BPSK over AWGN, Philox-4x32-10 channel generated on chip",
+        "config": {
+            "workload": f"matrix {code.name} (N={code.N}, M={code.n_checks}, P={code.P}, {code.n_edges} edges), "
+                        f"Eb/N0 2.5 and 3.0 dB, max 200 iterations, syndrome stop",
+            "kernel": kind, "storage": storage, "frames_per_point_per_gpu_per_step": F,
+            "parallelism": f"dp{world} (disjoint Philox frame ranges; tallies all-reduced)",
+            "l2": "flushed between steps (256 MiB write)",
+            "frames_per_s": round(tot_frames / dev_max, 1),
+            "points": {str(eb): {"frames": a["frames"], "frame_errors": a["fe"], "bit_errors": a["be"],
+                                 "mean_iters": round(a["iters"] / max(a["frames"], 1), 4)}
+                       for eb, a in acc.items()},
+        },
+        "e2e": {"value": round(tot_frames * code.n_tx / e2e_max / 1e9, 4), "unit": UNIT,
+                "h2d_bytes_per_step": int(len(POINTS) * (dec.launch_param_bytes + 64)),
+                "d2h_bytes_per_step": int(len(POINTS) * 64),
+                "path": "ldpc_run_chunk per Eb/N0 point (host params in, host tallies out)"},
+        "gpu_launches": int(tot_launches),
+        "roofline": {
+            "bound": "issue", "unit": "Tlane-op/s", "achieved": round(ops / dev_s / 1e12, 3),
+            "peak": round(peak, 3), "frac": round(ops / dev_s / 1e12 / peak, 4), "traffic": None,
+            "work": f"{LANE_OPS_PER_EDGE} lane-ops x {code.n_edges} edges x executed iterations",
+            "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz",
         },
         "clocks": clocks,
     }
@@ -821,6 +973,8 @@ def main():
         return run_mixed(args)
     if args.workload == "circulant":
         return run_circulant(args)
+    if args.workload == "file":
+        return run_file(args)
     return run_ours(args)
 
 
