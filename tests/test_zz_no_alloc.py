@@ -61,6 +61,29 @@ def test_static_matches_allocating_entry_on_makeh_code(storage, gpu):
     _check_same(c.row_matrix(), c.N, c.P, llr, max_iter=80, storage=storage)
 
 
+@pytest.mark.parametrize("storage", ["bf16", "fp32"])
+def test_static_matches_allocating_entry_and_oracle_on_random_ragged_matrices(storage, gpu):
+    """Random sparse matrices with ragged rows (degree 1 to 8: the degree-8 kernel and its two
+    16-byte column loads per row): the static entry (its row schedule built on the device), the
+    allocating one (schedule built on the host) and the oracle's serial file order agree bit for
+    bit."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(17 if storage == "bf16" else 18)
+    for N, M in ((300, 150), (512, 400)):
+        P = N // 10
+        rows = np.full((M, 8), -1, np.int32)
+        for m in range(M):
+            k = int(rng.integers(1, 9))
+            rows[m, :k] = rng.choice(N, size=k, replace=False)
+        llr = (1.2 + 1.6 * rng.standard_normal((24, N - P))).astype(np.float32)
+        _check_same(rows, N, P, llr, max_iter=30, storage=storage)
+        mode = O.STORE_BF16 if storage == "bf16" else O.STORE_FP32
+        opost, oit, osf, obe = O.decode(O.Code(rows, N, P), llr, mode=mode, max_iter=30)
+        spost, sit, ssf, sbe, _ = _static_decode(rows, N, P, llr, capi.Decoder.params(max_iter=30, storage=storage))
+        assert np.array_equal(spost.view(np.uint32), opost.view(np.uint32))
+        assert np.array_equal(sit, oit) and np.array_equal(ssf, osf) and np.array_equal(sbe, obe)
+
+
 def test_static_rejects_matrices_beyond_its_scratch(gpu):
     # 4 frame slots x (rows x degree) bf16 messages must fit 16 MiB: 1,200,000 rows of degree 4 do not
     M, d = 1_200_000, 4
