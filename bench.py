@@ -59,6 +59,7 @@ SM_COUNT = 148
 LANES_PER_SM = 128
 SMEM_BYTES_PER_CLK = 128
 PROFILE_SUMMARY = os.path.join(REPO, "profiles", "qc_decode_r12k1_fp32_ncu.txt")
+GENERAL_PROFILE = os.path.join(REPO, "profiles", "general_step_kernel_shipped_r12k1_bf16_ncu.txt")
 
 
 def log(*a):
@@ -84,6 +85,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-host-llr", action="store_true", help="skip the host-LLR decode figure")
     ap.add_argument("--no-compare", action="store_true", help="skip the other storage modes")
+    ap.add_argument("--no-file-workload", action="store_true",
+                    help="default line: skip the shipped matrix file's sub-record (config.file_workload)")
+    ap.add_argument("--no-mixed-workload", action="store_true",
+                    help="default line: skip the mixed-code batch's sub-record (config.mixed_workload)")
     ap.add_argument("--ref-step-seconds", type=float, default=2.0,
                     help="reference arm: CPU seconds per Eb/N0 point per step")
     return ap.parse_args()
@@ -115,6 +120,34 @@ def file_code(args):
     if not args.matrix:
         raise SystemExit("--workload file needs --matrix PATH")
     return FileCode(args.matrix, args.punctured)
+
+
+class RowsCode:
+    """A parity-check matrix given as its row table (file order, -1 padded)."""
+
+    def __init__(self, name: str, rows, N: int, P: int):
+        import numpy as np
+        self.rows = np.ascontiguousarray(rows, dtype=np.int32)
+        self.name, self.N, self.P = name, int(N), int(P)
+        self.n_checks = self.rows.shape[0]
+        self.n_tx = self.N - self.P
+        self.n_edges = int((self.rows >= 0).sum())
+
+    def row_matrix(self):
+        return self.rows
+
+
+SHIPPED_FIXTURE = os.path.join(REPO, "tests", "golden", "golden_scalar_worker.npz")
+
+
+def shipped_code():
+    """The reference's shipped matrix file (matrices/AR4JA_r45_4c_128c_r12.chinn.out, the file
+    CallSim.sh sends through run_simulation.py): the r1/2 K=1024 code with rows and columns permuted,
+    its rows as committed in the golden fixture, P = 512."""
+    import numpy as np
+    with np.load(SHIPPED_FIXTURE) as z:
+        rows = z["shipped_rows"].astype(np.int32)
+    return RowsCode("AR4JA_r45_4c_128c_r12.chinn.out", rows, 2560, 512)
 
 
 def mu_sigma(code, ebn0):
@@ -468,6 +501,20 @@ def run_ours(args):
             log(f"cpu baseline failed: {e}")
             cpu = None
 
+    # the two other workloads measured beside the headline (one GPU: a multi-rank run reports the
+    # headline only, every rank taking the same collective steps)
+    file_rec = mixed_rec = None
+    if world == 1 and not args.no_file_workload:
+        try:
+            file_rec = file_subrecord(args, local)
+        except Exception as e:
+            log(f"file workload failed: {e}")
+    if world == 1 and not args.no_mixed_workload:
+        try:
+            mixed_rec = mixed_subrecord(args, local)
+        except Exception as e:
+            log(f"mixed workload failed: {e}")
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -509,6 +556,8 @@ def run_ours(args):
             "storage_comparison": compare,
             "autotune": tuned,
             "wall_s": round(wall_max, 3),
+            "file_workload": file_rec,
+            "mixed_workload": mixed_rec,
         },
         "e2e": {"value": round(e2e, 4), "unit": UNIT,
                 "h2d_bytes_per_step": int(len(POINTS) * (dec.launch_param_bytes + 64)),
@@ -542,30 +591,13 @@ def run_ours(args):
     return 0
 
 
-def run_file(args):
-    """Any matrix file on one GPU (or independent replicas with disjoint frames): the drop-in engine's
-    decode path for that file, timed like the error-floor line."""
+def file_measure(dec, code, storage, F, warmup, steps, world=1, rank=0, dist=None, clock_gpus=()):
+    """Times `steps` steps of the file workload on `dec` (each step: F frames at each Eb/N0 point
+    through ldpc_run_chunk, L2 flushed between steps) after `warmup` untimed ones.  Returns the
+    per-point accumulators, the launches issued in the timed steps, and the clock summary."""
     import torch
 
-    from ldpcb200 import capi
     from ldpcb200.dist import frame_range
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    code = file_code(args)
-    dec = capi.Decoder(code.row_matrix(), code.N, code.P, local)
-    kind = "qc" if dec.kind == capi.KERNEL_QC else "general"
-    storage = "bf16" if args.storage == "auto" else args.storage
-    F = args.frames
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     def step(i, acc=None):
@@ -583,20 +615,119 @@ def run_file(args):
                 a["iters"] += r.iter_sum; a["kernel_ms"] += r.kernel_ms; a["e2e_s"] += t1 - t0
         flush.zero_()
 
-    for i in range(args.warmup):
+    for i in range(warmup):
         step(10_000 + i)
     acc = {eb: dict(frames=0, fe=0, be=0, iters=0, kernel_ms=0.0, e2e_s=0.0) for eb in POINTS}
     launches0 = dec.launches
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(list(range(world)) if rank == 0 else []) as clk:
-        for i in range(args.steps):
+    with ClockSampler(list(clock_gpus)) as clk:
+        for i in range(steps):
             step(i, acc)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-    launches = dec.launches - launches0
+    return acc, dec.launches - launches0, clk.summary()
+
+
+def general_traffic(frames_per_launch):
+    """DRAM bytes of one general step-kernel launch of `frames_per_launch` frames: the committed ncu
+    capture (line 'dram_bytes_per_frame: X' of the step kernel's summary) scaled by the frames."""
+    try:
+        with open(GENERAL_PROFILE) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_frame:"):
+                    return round(float(line.split(":")[1]) * frames_per_launch)
+    except OSError:
+        pass
+    return None
+
+
+def file_roofline(code, iters, dev_s, clocks, frames_per_launch=None):
+    f_mhz = clocks["sm_mhz"] if clocks else measured_peaks().get("sm_max_mhz", 1965.0)
+    ops = LANE_OPS_PER_EDGE * code.n_edges * iters
+    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
+    return {
+        "bound": "issue", "unit": "Tlane-op/s", "achieved": round(ops / dev_s / 1e12, 3),
+        "peak": round(peak, 3), "frac": round(ops / dev_s / 1e12 / peak, 4),
+        "traffic": general_traffic(frames_per_launch) if frames_per_launch else None,
+        "work": f"{LANE_OPS_PER_EDGE} lane-ops x {code.n_edges} edges x executed iterations",
+        "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz",
+    }
+
+
+def file_subrecord(args, local):
+    """The drop-in path's default matrix (the reference's shipped permuted file, which
+    run_simulation.py decodes through the general kernel), measured beside the headline: launch
+    shape autotuned in bf16 (the reference numerics), 3 warm-up and 2-4 timed steps of the same
+    frames per point, the reference's decoder on the same matrix as its CPU baseline."""
+    from ldpcb200 import capi
+    code = shipped_code()
+    dec = capi.Decoder(code.row_matrix(), code.N, code.P, local)
+    try:
+        mu, sigma = mu_sigma(code, POINTS[0])
+        res, _ = dec.autotune(mu, sigma, storages=("bf16",), frames=1 << 18)
+        shape, timings = res["bf16"]
+        steps = max(2, min(args.steps, 4))
+        acc, launches, clocks = file_measure(dec, code, "bf16", args.frames, 3, steps, clock_gpus=(local,))
+        dev_s = sum(a["kernel_ms"] for a in acc.values()) / 1e3
+        e2e_s = sum(a["e2e_s"] for a in acc.values())
+        frames = sum(a["frames"] for a in acc.values())
+        iters = sum(a["iters"] for a in acc.values())
+        rec = {
+            "workload": f"matrix {code.name} (N={code.N}, M={code.n_checks}, P={code.P}, {code.n_edges} edges; "
+                        "rows and columns permuted, so the general kernel in file order), Eb/N0 2.5 and 3.0 dB, "
+                        "max 200 iterations, syndrome stop, bf16 reference numerics",
+            "value": round(frames * code.n_tx / dev_s / 1e9, 4), "unit": UNIT,
+            "frames_per_s": round(frames / dev_s, 1), "steps": steps, "warmup": 3,
+            "kernel": "general_step_kernel" if shape[3] == 3 else "general_kernel (warp)",
+            "shape": list(shape), "autotune_mframes_per_s": {",".join(map(str, k)): round(v, 3)
+                                                              for k, v in timings.items()},
+            "points": {str(eb): {"frames": a["frames"], "frame_errors": a["fe"], "bit_errors": a["be"],
+                                 "mean_iters": round(a["iters"] / max(a["frames"], 1), 4)}
+                       for eb, a in acc.items()},
+            "e2e": {"value": round(frames * code.n_tx / e2e_s / 1e9, 4), "unit": UNIT,
+                    "path": "ldpc_run_chunk per Eb/N0 point (host params in, host tallies out)"},
+            "gpu_launches": int(launches),
+            "roofline": file_roofline(code, iters, dev_s, clocks, args.frames),
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline:
+            try:
+                rec["cpu_baseline"] = cpu_baseline(args.cpu_seconds / 2, code=code)
+            except Exception as e:
+                log(f"file-workload cpu baseline failed: {e}")
+        return rec
+    finally:
+        dec.close()
+
+
+def run_file(args):
+    """Any matrix file on one GPU (or independent replicas with disjoint frames): the drop-in engine's
+    decode path for that file, timed like the error-floor line."""
+    import torch
+
+    from ldpcb200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    code = file_code(args)
+    dec = capi.Decoder(code.row_matrix(), code.N, code.P, local)
+    kind = "qc" if dec.kind == capi.KERNEL_QC else "general"
+    storage = "bf16" if args.storage == "auto" else args.storage
+    F = args.frames
+    acc, launches, clocks = file_measure(dec, code, storage, F, args.warmup, args.steps, world, rank, dist,
+                                         range(world) if rank == 0 else ())
     dev_s = sum(a["kernel_ms"] for a in acc.values()) / 1e3
     e2e_s = sum(a["e2e_s"] for a in acc.values())
     frames = sum(a["frames"] for a in acc.values())
@@ -620,10 +751,6 @@ def run_file(args):
     if rank != 0:
         dec.close()
         return 0
-    clocks = clk.summary()
-    f_mhz = clocks["sm_mhz"] if clocks else measured_peaks().get("sm_max_mhz", 1965.0)
-    ops = LANE_OPS_PER_EDGE * code.n_edges * iters
-    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
     line = {
         "metric": METRIC, "value": round(tot_frames * code.n_tx / dev_max / 1e9, 4), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -646,12 +773,7 @@ def run_file(args):
                 "d2h_bytes_per_step": int(len(POINTS) * 64),
                 "path": "ldpc_run_chunk per Eb/N0 point (host params in, host tallies out)"},
         "gpu_launches": int(tot_launches),
-        "roofline": {
-            "bound": "issue", "unit": "Tlane-op/s", "achieved": round(ops / dev_s / 1e12, 3),
-            "peak": round(peak, 3), "frac": round(ops / dev_s / 1e12 / peak, 4), "traffic": None,
-            "work": f"{LANE_OPS_PER_EDGE} lane-ops x {code.n_edges} edges x executed iterations",
-            "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz",
-        },
+        "roofline": file_roofline(code, iters, dev_s, clocks, F if kind == "general" else None),
         "clocks": clocks,
     }
     if cpu:
@@ -659,6 +781,87 @@ def run_file(args):
     print(json.dumps(line), flush=True)
     dec.close()
     return 0
+
+
+def mixed_measure(wl, total, warmup, steps, world=1, rank=0, warm_frames=None, clock_gpus=()):
+    """Times `steps` graph launches of the mixed workload (`total` frames each, split over the nine
+    codes, L2 flushed between launches) after `warmup` untimed launches of `warm_frames` frames."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(i, n):
+        res, ms = wl.run(n, seed=SEED, first_frame=(i * world + rank) * total)
+        flush.zero_()
+        return res, ms
+
+    for i in range(warmup):
+        step(1_000_000 + i, warm_frames or total)
+    torch.cuda.synchronize()
+    launches0 = sum(d.launches for d in wl.decs)
+    out = dict(dev_ms=0.0, e2e_s=0.0, frames=0, symbols=0, lane_ops=0, per_code={})
+    with ClockSampler(list(clock_gpus)) as clk:
+        for i in range(steps):
+            t0 = time.perf_counter()
+            res, ms = step(i, total)
+            out["e2e_s"] += time.perf_counter() - t0
+            out["dev_ms"] += ms
+            for c, r in zip(wl.codes, res):
+                out["frames"] += r.frames
+                out["symbols"] += r.frames * r.n_tx
+                out["lane_ops"] += LANE_OPS_PER_EDGE * c.n_edges * r.iter_sum
+                a = out["per_code"].setdefault(r.name, {"frames": 0, "frame_errors": 0, "iters": 0})
+                a["frames"] += r.frames; a["frame_errors"] += r.frame_errors; a["iters"] += r.iter_sum
+        torch.cuda.synchronize()
+    out["launches"] = sum(d.launches for d in wl.decs) - launches0
+    out["clocks"] = clk.summary()
+    return out
+
+
+MIXED_WORKLOAD = ("mixed: nine AR4JA codes (K 1024/4096/16384 x rate 1/2, 2/3, 4/5), frames split uniformly "
+                  "over codes, per-frame Eb/N0 uniform in [thr+0.5, thr+2.0] dB, max 200 iterations, one "
+                  "CUDA-graph launch per step")
+
+
+def mixed_roofline(lane_ops, dev_s, clocks):
+    f_mhz = clocks["sm_mhz"] if clocks else measured_peaks().get("sm_max_mhz", 1965.0)
+    achieved = lane_ops / dev_s / 1e12
+    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
+    return {"bound": "issue", "unit": "Tlane-op/s", "achieved": round(achieved, 3), "peak": round(peak, 3),
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "work": f"{LANE_OPS_PER_EDGE} lane-ops x edges x executed iterations, summed over codes",
+            "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz"}
+
+
+def mixed_codes(wl, per_code):
+    return {n: {"frames": v["frames"], "fer": v["frame_errors"] / max(v["frames"], 1),
+                "mean_iters": round(v["iters"] / max(v["frames"], 1), 3)} for n, v in per_code.items()}
+
+
+def mixed_tuning(wl):
+    return {c.name: {"storage": st, "shape": list(sh), "mframes_per_s_alone": round(f / 1e6, 4)}
+            for c, st, sh, f in zip(wl.codes, wl.storage, wl.shape, wl.rate_fps)}
+
+
+def mixed_subrecord(args, local):
+    """Config 3's batched mixed-code launch beside the headline: the nine codes autotuned, 3 warm-up
+    launches of 2^20 frames, then 2 timed launches of --mixed-frames (2^24) frames."""
+    from ldpcb200 import mixed
+    wl = mixed.MixedWorkload(device=local)
+    try:
+        m = mixed_measure(wl, args.mixed_frames, 3, 2, warm_frames=1 << 20, clock_gpus=(local,))
+        dev_s = m["dev_ms"] / 1e3
+        return {
+            "workload": MIXED_WORKLOAD, "frames_per_launch": args.mixed_frames, "steps": 2, "warmup": 3,
+            "value": round(m["symbols"] / dev_s / 1e9, 4), "unit": UNIT,
+            "frames_per_s": round(m["frames"] / dev_s, 1), "graph_ms_per_launch": round(m["dev_ms"] / 2, 2),
+            "e2e": {"value": round(m["symbols"] / m["e2e_s"] / 1e9, 4), "unit": UNIT,
+                    "path": "ldpc_batch_run per launch (host params in, host tallies out)"},
+            "gpu_launches": int(m["launches"]),
+            "roofline": mixed_roofline(m["lane_ops"], dev_s, m["clocks"]),
+            "codes": mixed_codes(wl, m["per_code"]), "tuning": mixed_tuning(wl), "clocks": m["clocks"],
+        }
+    finally:
+        wl.close()
 
 
 def run_mixed(args):
@@ -679,39 +882,12 @@ def run_mixed(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     wl = mixed.MixedWorkload(device=local)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     total = args.mixed_frames
-
-    def step(i):
-        res, ms = wl.run(total, seed=SEED, first_frame=(i * world + rank) * total)
-        flush.zero_()
-        return res, ms
-
-    for i in range(args.warmup):
-        step(1_000_000 + i)
-    torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    launches0 = sum(d.launches for d in wl.decs)
-    dev_ms = e2e_s = 0.0
-    frames = symbols = lane_ops = 0
-    per_code = {}
-    with ClockSampler(list(range(world)) if rank == 0 else []) as clk:
-        for i in range(args.steps):
-            t0 = time.perf_counter()
-            res, ms = step(i)
-            e2e_s += time.perf_counter() - t0
-            dev_ms += ms
-            for c, r in zip(wl.codes, res):
-                frames += r.frames
-                symbols += r.frames * r.n_tx
-                lane_ops += LANE_OPS_PER_EDGE * c.n_edges * r.iter_sum
-                a = per_code.setdefault(r.name, {"frames": 0, "frame_errors": 0, "iters": 0})
-                a["frames"] += r.frames; a["frame_errors"] += r.frame_errors; a["iters"] += r.iter_sum
-        torch.cuda.synchronize()
-    launches = sum(d.launches for d in wl.decs) - launches0
-    vals = torch.tensor([dev_ms / 1e3, e2e_s], dtype=torch.float64, device="cuda")
-    cnt = torch.tensor([frames, symbols, launches], dtype=torch.float64, device="cuda")
+    m = mixed_measure(wl, total, args.warmup, args.steps, world, rank, clock_gpus=range(world) if rank == 0 else ())
+    vals = torch.tensor([m["dev_ms"] / 1e3, m["e2e_s"]], dtype=torch.float64, device="cuda")
+    cnt = torch.tensor([m["frames"], m["symbols"], m["launches"]], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
         dist.all_reduce(cnt, op=dist.ReduceOp.SUM)
@@ -721,11 +897,6 @@ def run_mixed(args):
     if rank != 0:
         wl.close()
         return 0
-    clocks = clk.summary()
-    peaks = measured_peaks()
-    f_mhz = clocks["sm_mhz"] if clocks else peaks.get("sm_max_mhz", 1965.0)
-    achieved = lane_ops / (dev_ms / 1e3) / 1e12
-    peak = SM_COUNT * LANES_PER_SM * f_mhz * 1e6 / 1e12
     line = {
         "metric": METRIC, "value": round(tot_symbols / dev_s / 1e9, 4), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dev_s / args.steps, 3),
@@ -733,27 +904,20 @@ def run_mixed(args):
         "data": "synthetic: all-zero codeword, BPSK over AWGN, Philox-4x32-10 channel generated on chip, "
                 "per-frame Eb/N0",
         "config": {
-            "workload": "mixed: nine AR4JA codes (K 1024/4096/16384 x rate 1/2, 2/3, 4/5), frames split "
-                        "uniformly over codes, per-frame Eb/N0 uniform in [thr+0.5, thr+2.0] dB, max 200 "
-                        "iterations, one CUDA-graph launch per step",
+            "workload": MIXED_WORKLOAD,
             "frames_per_step_per_gpu": total, "frames_per_s": round(tot_frames / dev_s, 1),
             "parallelism": f"{world} independent replicas (disjoint frame ranges)",
             "l2": "flushed between steps (256 MiB write); inputs generated on chip",
-            "codes": {n: {"frames": v["frames"], "fer": v["frame_errors"] / max(v["frames"], 1),
-                          "mean_iters": round(v["iters"] / max(v["frames"], 1), 3)} for n, v in per_code.items()},
-            "tuning": {c.name: {"storage": st, "shape": list(sh), "mframes_per_s_alone": round(f / 1e6, 4)}
-                       for c, st, sh, f in zip(wl.codes, wl.storage, wl.shape, wl.rate_fps)},
+            "codes": mixed_codes(wl, m["per_code"]),
+            "tuning": mixed_tuning(wl),
         },
         "e2e": {"value": round(tot_symbols / e2e_max / 1e9, 4), "unit": UNIT,
                 "h2d_bytes_per_step": int(len(wl.codes) * (wl.decs[0].launch_param_bytes + 64)),
                 "d2h_bytes_per_step": int(len(wl.codes) * 64),
                 "path": "ldpc_batch_run per step (host params in, host tallies out)"},
         "gpu_launches": int(tot_launches),
-        "roofline": {"bound": "issue", "unit": "Tlane-op/s", "achieved": round(achieved, 3), "peak": round(peak, 3),
-                     "frac": round(achieved / peak, 4), "traffic": None,
-                     "work": f"{LANE_OPS_PER_EDGE} lane-ops x edges x executed iterations, summed over codes",
-                     "peak_source": f"{SM_COUNT} SMs x {LANES_PER_SM} lanes x {f_mhz:.0f} MHz"},
-        "clocks": clocks,
+        "roofline": mixed_roofline(m["lane_ops"], m["dev_ms"] / 1e3, m["clocks"]),
+        "clocks": m["clocks"],
     }
     print(json.dumps(line), flush=True)
     wl.close()

@@ -367,16 +367,20 @@ int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCod
     if (cudaMemcpy(g->d_cols, cols.data(), cols.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(g->d_runs, runs.data(), runs.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
         return gfail(err, LDPC_EIO, "copy of the matrix to the device failed");
-    return 0;
+    return build_general_steps(rows, dmax, order, runs, g, err);
 }
 
 void free_general(GeneralCode* g) {
     cudaFree(g->d_cols);
     cudaFree(g->d_runs);
     cudaFree(g->d_r);
+    cudaFree(g->d_scols[0]);
+    cudaFree(g->d_scols[1]);
     g->d_cols = g->d_runs = nullptr;
+    g->d_scols[0] = g->d_scols[1] = nullptr;
     g->d_r = nullptr;
     g->r_cap = 0;
+    g->sdt = 0;
 }
 
 template <int DT, int MODE, int ALGO, bool EXT, int NW = GEN_WARPS>

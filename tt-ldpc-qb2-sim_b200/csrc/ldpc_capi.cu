@@ -362,13 +362,30 @@ extern "C" int ldpc_set_circulant(ldpc_handle* h, const ldpc_circ_config* c) {
     return 0;
 }
 
+// Shapes of the general kernels (layouts 3 and 4 of ldpc_set_launch_shape).
+static bool general_shape_ok(const ldpc_handle* h, int R, int F, int B, int G) {
+    if (G == GEN_LAYOUT_STEP) return R == 1 && F == 1 && B >= 0 && B <= 32 && h->gen.sdt > 0;
+    return G == GEN_LAYOUT_WARP && R == 1 && F == GEN_WARPS && B == 0;
+}
+
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
-    if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "launch shapes apply to the QC kernel");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 2)
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 4)
         return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
+    if (h->kind != LDPC_KERNEL_QC) {
+        if (!reset && !general_shape_ok(h, R, F, B, G))
+            return fail(LDPC_ENOTSUP, "shape R=%d F=%d B=%d G=%d not built for this general matrix", R, F, B, G);
+        for (int s = lo; s <= hi; ++s) {
+            h->shape[s][0] = R;
+            h->shape[s][1] = F;
+            h->shape[s][2] = B;
+            h->shape[s][3] = G;
+        }
+        return 0;
+    }
+    if (G > 2) return fail(LDPC_ENOTSUP, "layouts 3 and 4 are the general kernels'");
     bool any = reset;
     auto built = [&](int s) {
         return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G) ||
@@ -390,8 +407,22 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
 extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo, int32_t* shapes, int max_shapes) {
     if (!h || storage < 0 || storage > 2 || algo < 0 || algo > 3 || (max_shapes > 0 && !shapes))
         return fail(LDPC_EINVAL, "bad arguments");
-    if (h->kind != LDPC_KERNEL_QC) return 0;
     int n = 0;
+    if (h->kind != LDPC_KERNEL_QC) {
+        if (algo != LDPC_ALGO_AMIN && algo != LDPC_ALGO_NMS) return 0;
+        // the step kernel at every resident-CTA count worth timing, and the warp kernel
+        static const int32_t step_ctas[] = {0, 24, 16};
+        int32_t list[4][4];
+        if (h->gen.sdt)
+            for (int32_t b : step_ctas) {
+                list[n][0] = 1; list[n][1] = 1; list[n][2] = b; list[n][3] = GEN_LAYOUT_STEP;
+                ++n;
+            }
+        list[n][0] = 1; list[n][1] = GEN_WARPS; list[n][2] = 0; list[n][3] = GEN_LAYOUT_WARP;
+        ++n;
+        for (int i = 0; i < n && i < max_shapes; ++i) std::copy(list[i], list[i] + 4, shapes + 4 * i);
+        return n;
+    }
     for (const QcTable* t = qc_tables(); t; t = t->next)
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
@@ -644,8 +675,17 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
                 if ((rc = build_general(h->rows.data(), h->N, h->M, h->P, h->dmax, &h->gen, g_err)) != 0) return rc;
                 h->gen_built = true;
             }
-            rc = launch_general(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be, h->d_tally,
-                                h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err, h->d_snr);
+            // the step kernel unless the shape asks for the warp kernel (or the step kernel does not
+            // run these numerics / this matrix)
+            const int* sh = h->shape[p->storage];
+            h->gen.step_ctas = sh[3] == GEN_LAYOUT_STEP ? sh[2] : 0;
+            if (sh[3] != GEN_LAYOUT_WARP)
+                rc = launch_general_step(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be,
+                                         h->d_tally, h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err,
+                                         h->d_snr);
+            if (rc == LDPC_ENOTSUP)
+                rc = launch_general(&h->gen, p, ext, cnt, p->first_frame + off, llr, post, it, sf, be, h->d_tally,
+                                    h->d_hist, h->hist_bins, h->d_work, h->n_sm, h->stream, g_err, h->d_snr);
             if (!rc) h->launches++;
         }
         if (rc) return rc;

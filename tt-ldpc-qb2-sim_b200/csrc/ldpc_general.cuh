@@ -22,12 +22,22 @@ namespace ldpcb200 {
 
 constexpr int GEN_WARPS = 4;  // frame slots (warps) per CTA
 
+// Kernels for a general matrix: the step kernel (general_step.cu) when the matrix's degree allows
+// it and the numerics are ones it runs, else the warp kernel (general.cu).
+// Layout numbers of the two kernels in ldpc_set_launch_shape (0-2 are the QC kernel's layouts).
+enum GenLayout : int { GEN_LAYOUT_STEP = 3, GEN_LAYOUT_WARP = 4 };
+
 struct GeneralCode {
     int N = 0, M = 0, P = 0, dmax = 0, n_runs = 0, dt = 0;  // dt: compiled degree bound
     int32_t* d_cols = nullptr;  // [M][gen_dtc(dt)] columns of the row at schedule position k (-1 pad)
     int32_t* d_runs = nullptr;  // [n_runs + 1] first position of each step, then M
-    void* d_r = nullptr;        // message scratch: [slots][M][gen_dtr(dt)] elements
+    void* d_r = nullptr;        // message scratch of either kernel (one slot per resident frame)
     size_t r_cap = 0;
+    // step kernel: the same steps, each padded to 32 rows (lane j takes row j of the step); a lane
+    // without a row and an edge past its row's degree point at the dummy posterior slot N
+    int sdt = 0;                          // its degree bound (0: the matrix needs the warp kernel)
+    int32_t* d_scols[2] = {nullptr, nullptr};  // byte offsets for 2- and 4-byte posteriors, step_table layout
+    int step_ctas = 0;                    // step kernel CTAs per SM (0: as many as fit)
 };
 
 struct GenParams {
@@ -50,6 +60,8 @@ struct GenParams {
     unsigned int* work;
     float ebn0_lo, ebn0_hi, rate;         // per-frame Eb/N0 (see QcParams)
     unsigned long long* snr_bins;
+    const int32_t* scols;                 // step kernel: its column table (byte offsets)
+    int32_t n_steps;
 };
 
 void general_schedule(const int32_t* rows, int N, int M, int dmax, std::vector<int32_t>& order,
@@ -60,6 +72,15 @@ void free_general(GeneralCode* g);
 int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr, int64_t n,
                       float* d_post, int32_t* d_iters, int32_t* d_synd, int32_t* d_be, ldpc_tally* out,
                       cudaStream_t stream, std::string& err);
+// Builds the step kernel's tables for the schedule (order, starts) of build_general.
+int build_general_steps(const int32_t* rows, int dmax, const std::vector<int32_t>& order,
+                        const std::vector<int32_t>& starts, GeneralCode* g, std::string& err);
+// The step kernel; LDPC_ENOTSUP when it does not run these numerics or this matrix (the caller then
+// takes the warp kernel).
+int launch_general_step(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
+                        const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
+                        unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,
+                        int n_sm, cudaStream_t stream, std::string& err, unsigned long long* d_snr_bins);
 int launch_general(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,
                    const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                    unsigned long long* d_tally, unsigned long long* d_hist, int hist_bins, unsigned int* d_work,

@@ -183,7 +183,12 @@ template <int d, int MODE> struct RowMsgGlobal {
 // iteration (edge e at wt[f][e]: a constant offset, no class lookup).
 // BO: idx[e] holds byte offsets into the slot's L array instead of element indices (the column
 // offset table of the OT layout), so no index scaling is needed.
-template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG, bool BO = false>
+// PAD: rows of a smaller degree padded to d with edges whose posterior is the largest finite value
+// (the general step kernel): such an edge is never the minimum and a min* step with it returns the
+// other operand unchanged, so only a row with fewer than two real edges needs care: its chain over
+// the other edges then holds no real value (above 1e38), and the reference's m_others is the row's
+// minimum (ldpc_decoder_core.h:180-181).
+template <int d, int MODE, int ALGO, bool CLIP, int F, class MSG, bool BO = false, bool PAD = false>
 __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits<MODE>::T* sL, int lstride,
                                            MSG (&rm)[F], float r_cap, float lp_cap,
                                            const float2* const* wt = nullptr) {
@@ -231,6 +236,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
             float m = lt[0] ? a[0] : a[1];
 #pragma unroll
             for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, lt[i] ? a[i] : a[i + 1]);
+            if (PAD) m = m > 1e38f ? mn : m;
             mag_min = m;
             mag_all = amin_step_fma(m, mn);
         } else {

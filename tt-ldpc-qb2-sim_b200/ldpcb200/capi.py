@@ -262,8 +262,10 @@ class Decoder:
                                                global_messages))
 
     def shapes(self, storage, algo: int = ALGO_AMIN) -> list:
-        """Built QC launch shapes (rows per thread, frames per CTA, min CTAs per SM, global messages)
-        for a storage mode and algorithm."""
+        """Built launch shapes (rows per thread, frames per CTA, min CTAs per SM, layout) for a
+        storage mode and algorithm: the QC kernel's, or for a general matrix the step kernel's
+        (layout 3; third entry = resident CTAs per SM, 0 = as many as fit) and the warp kernel's
+        (layout 4)."""
         if isinstance(storage, str):
             storage = STORAGE_NAMES[storage]
         buf = np.zeros(4 * 64, np.int32)
@@ -278,7 +280,7 @@ class Decoder:
         out = {}
         best_overall = None
         for st in storages:
-            shapes = self.shapes(st, algo) if self.kind == KERNEL_QC else []
+            shapes = self.shapes(st, algo)
             timings = {}
             for sh in shapes:
                 self.set_launch_shape(*sh, storage=st)
