@@ -217,6 +217,19 @@ def mc_pairs(code: Code, max_iter: int, mu: float, sigma: float, state: np.ndarr
 
 # --------------------------- the reference's own binaries (oracle/_ref) ---------------------------
 
+def reference_tree() -> str:
+    """The reference checkout this test infrastructure reads: LDPC_REFERENCE_TREE, else the one the
+    oracle recipe names (``make -s -C oracle print-ref``); "" when neither answers."""
+    t = os.environ.get("LDPC_REFERENCE_TREE", "")
+    if t:
+        return t
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True, timeout=60)
+        return r.stdout.strip() if r.returncode == 0 else ""
+    except (OSError, subprocess.SubprocessError):
+        return ""
+
+
 def ref_binary(name: str) -> Optional[str]:
     p = os.path.join(REF_DIR, name)
     return p if os.path.exists(p) and os.access(p, os.X_OK) else None

@@ -11,7 +11,9 @@ for p in (REPO, SRC):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(REPO, "tests", "golden", "golden_scalar_worker.npz")
-REFERENCE = os.environ.get("LDPC_REFERENCE_TREE", "/root/reference")
+from oracle.oracle import reference_tree  # noqa: E402
+
+REFERENCE = reference_tree()  # the reference checkout, "" when absent (tests that need it skip)
 
 
 def n_golden_cases() -> int:

@@ -24,7 +24,9 @@ from ldpcb200 import ar4ja, chinn  # noqa: E402
 from ldpcb200.capi import channel_mu_sigma  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else O.reference_tree()
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("the reference tree is needed: pass its path or set LDPC_REFERENCE_TREE")
 SHIPPED = len(sys.argv) > 2 and sys.argv[2] == "shipped"
 POINTS = [0.5, 0.75, 1.0, 1.25, 1.5, 1.75, 2.0]
 FRAMES = 10000

@@ -20,7 +20,9 @@ sys.path.insert(0, REPO)
 
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else O.reference_tree()
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("the reference tree is needed: pass its path or set LDPC_REFERENCE_TREE")
 POINTS = [0.75, 1.0, 1.25, 1.5, 1.75]
 FRAMES = 20000
 

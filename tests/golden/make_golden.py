@@ -3,7 +3,7 @@
 Runs run_ldpc_worker (engines/scalar_5w/ldpc_decoder_core.h:214-586), compiled from the reference's
 sources by ``make -C oracle ref`` (oracle/ref_golden.cpp), and records for every codeword pair the
 packed bf16 channel LLRs it decoded and the packed bf16 buffer it left behind, with its stats.  Needs
-the reference tree (REF, default /root/reference); the committed fixtures are what the tests read.
+the reference tree (REF: the argument, else LDPC_REFERENCE_TREE or the oracle recipe's print-ref); the committed fixtures are what the tests read.
 
     python tests/golden/make_golden.py [REF]
 """
@@ -22,7 +22,9 @@ from ldpcb200 import ar4ja, chinn  # noqa: E402
 from ldpcb200.capi import channel_mu_sigma  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else O.reference_tree()
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("the reference tree is needed: pass its path or set LDPC_REFERENCE_TREE")
 SHIPPED = os.path.join(REF, "matrices", "AR4JA_r45_4c_128c_r12.chinn.out")
 
 

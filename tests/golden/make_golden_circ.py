@@ -5,7 +5,7 @@ Runs step_tile_circulant_dma_scalar / step_tile_circulant_dma_sfpu
 sources by ``make -C oracle ref`` (oracle/ref_circ.cpp), on groups of 4 codewords of AR4JA rate 1/2,
 K = 1024, and records the bf16 channel LLRs it decoded, the bf16 nodes it left behind, and its
 iteration count, frame-error flag and bit-error count per codeword.  Needs the reference tree (REF,
-default /root/reference); the committed fixture is what the tests read.
+the argument, else LDPC_REFERENCE_TREE or the oracle recipe's print-ref); the committed fixture is what the tests read.
 
     python tests/golden/make_golden_circ.py [REF]
 """
@@ -21,7 +21,9 @@ sys.path.insert(0, REPO)
 
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else O.reference_tree()
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("the reference tree is needed: pass its path or set LDPC_REFERENCE_TREE")
 
 # (Eb/N0 dB, sfpu, damping, max_iter): both arithmetic forms, the device engine's damping 15/16,
 # iteration caps that leave frames unconverged (bit errors counted) and ones that let them converge.

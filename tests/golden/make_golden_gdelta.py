@@ -5,7 +5,7 @@ reference: the two-line min* of the circulant engine), compiled from the referen
 ``make -C oracle ref`` (oracle/ref_gdelta.cpp), on the unit test's own sweep (a = 10, b = a + d for
 2001 d in [0, 6]), on corner cases (zeros, equal inputs, d at the 0.5 and 2 region edges and at the
 line crossing, tiny and large magnitudes) and on 8000 seeded random pairs.  Needs the reference tree
-(REF, default /root/reference); the committed fixture is what the tests read.
+(REF: the argument, else LDPC_REFERENCE_TREE or the oracle recipe's print-ref); the committed fixture is what the tests read.
 
     python tests/golden/make_golden_gdelta.py [REF]
 """
@@ -21,7 +21,9 @@ sys.path.insert(0, REPO)
 
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else O.reference_tree()
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("the reference tree is needed: pass its path or set LDPC_REFERENCE_TREE")
 
 
 def main():

@@ -92,3 +92,16 @@ def test_static_rejects_matrices_beyond_its_scratch(gpu):
     with pytest.raises(capi.LdpcError) as e:
         capi.decode_llr_static(rows, 4096, 0, p, 0, 0)
     assert e.value.code == -12 and "static scratch" in str(e.value)
+
+
+def test_static_one_slot_ctas_for_large_frames(gpu):
+    """Frames whose bf16 posteriors are too large for four to share a CTA (N = 24000: 4 x 48 KB) run
+    in one-slot CTAs, as ldpc_decode_llr runs them, with the same bits."""
+    rng = np.random.default_rng(23)
+    N, M, P = 24000, 12000, 2400
+    rows = np.full((M, 6), -1, np.int32)
+    for m in range(M):
+        k = int(rng.integers(3, 7))
+        rows[m, :k] = rng.choice(N, size=k, replace=False)
+    llr = (1.5 + 1.5 * rng.standard_normal((6, N - P))).astype(np.float32)
+    _check_same(rows, N, P, llr, max_iter=12, storage="bf16")

@@ -608,7 +608,7 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
                       cudaStream_t stream, std::string& err) {
     char msg[256];
     if (!h || !h->rows || !p) return sfail(LDPC_EINVAL, err, "matrix or params are NULL");
-    if (n < 0 || n > (int64_t)UINT32_MAX) return sfail(LDPC_EINVAL, err, "n_frames out of range");
+    if (n < 0) return sfail(LDPC_EINVAL, err, "n_frames out of range");
     if (n > 0 && !d_llr) return sfail(LDPC_EINVAL, err, "d_llr is NULL");
     const int N = h->n_vars, M = h->n_checks, P = h->n_punct, dmax = h->max_check_deg;
     if (N <= 0 || M <= 0 || dmax <= 0 || dmax > 32 || P < 0 || P >= N)
@@ -626,6 +626,9 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     const int dt = maxdeg <= 6 ? 6 : maxdeg <= 8 ? 8 : maxdeg <= 20 ? 20 : 32;
     const int dtc = gen_dtc(dt);
     const size_t esz = p->storage == STORE_BF16 ? 2 : 4;
+    // frame slots per CTA as ldpc_decode_llr's warp kernel takes them: four while their posteriors fit
+    // comfortably in shared memory, else one
+    const int nw = (size_t)GEN_WARPS * ((N + 7) & ~7) * esz <= 160 * 1024 ? GEN_WARPS : 1;
     const size_t off_rows = 256;
     const size_t off_cols = off_rows + align256((size_t)M * dmax * 4);
     const size_t off_runs = off_cols + align256((size_t)M * dtc * 4);
@@ -636,10 +639,10 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
     const size_t off_cnt = off_order + align256((size_t)M * 4);
     const size_t off_msgs = off_cnt + align256((size_t)(M + 2) * 4);
     const size_t per_slot = gen_slot_bytes(M, dt, p->storage);
-    if (off_msgs + GEN_WARPS * per_slot > LDPC_STATIC_SCRATCH_BYTES) {
+    if (off_msgs + nw * per_slot > LDPC_STATIC_SCRATCH_BYTES) {
         snprintf(msg, sizeof msg,
                  "matrix needs %zu bytes of static scratch for one CTA of %d frame slots; the maximum is %zu",
-                 off_msgs + GEN_WARPS * per_slot, GEN_WARPS, (size_t)LDPC_STATIC_SCRATCH_BYTES);
+                 off_msgs + nw * per_slot, nw, (size_t)LDPC_STATIC_SCRATCH_BYTES);
         return sfail(LDPC_ENOMEM, err, msg);
     }
     int dev = 0;
@@ -662,23 +665,31 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         }
         base = g_static_addr[dev];
     }
-    const void* fn = dt == 6 ? pick_mode<6>(p->storage, p->algo, true)
-                   : dt == 8 ? pick_mode<8>(p->storage, p->algo, true)
-                   : dt == 20 ? pick_mode<20>(p->storage, p->algo, true)
-                              : pick_mode<32>(p->storage, p->algo, true);
-    const size_t smem = (size_t)GEN_WARPS * ((N + 7) & ~7) * esz;
+    const void* fn = nw == GEN_WARPS ? (dt == 6    ? pick_mode<6>(p->storage, p->algo, true)
+                                        : dt == 8  ? pick_mode<8>(p->storage, p->algo, true)
+                                        : dt == 20 ? pick_mode<20>(p->storage, p->algo, true)
+                                                   : pick_mode<32>(p->storage, p->algo, true))
+                                     : (dt == 6    ? pick_mode<6, 1>(p->storage, p->algo, true)
+                                        : dt == 8  ? pick_mode<8, 1>(p->storage, p->algo, true)
+                                        : dt == 20 ? pick_mode<20, 1>(p->storage, p->algo, true)
+                                                   : pick_mode<32, 1>(p->storage, p->algo, true));
+    const size_t smem = (size_t)nw * ((N + 7) & ~7) * esz;
     if (smem > 48 * 1024 && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return sfail(LDPC_ENOTSUP, err, "frame too large for shared memory");
     }
     int per_sm = 0, n_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * GEN_WARPS, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * nw, smem) != cudaSuccess ||
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0) {
         cudaGetLastError();
         return sfail(LDPC_ENOTSUP, err, "general kernel does not fit on an SM");
     }
-    const uint64_t fit = (LDPC_STATIC_SCRATCH_BYTES - off_msgs) / (GEN_WARPS * per_slot);
-    const uint64_t grid = std::min<uint64_t>({((uint64_t)n + GEN_WARPS - 1) / GEN_WARPS,
+    // The kernel claims frames with a 32-bit counter (and every warp makes one claim past the last
+    // frame), so a call decodes its frames in launches of at most 2^31, the counter re-zeroed between
+    // them and the tallies summed across them.
+    constexpr uint64_t kLaunchFrames = 1ull << 31;
+    const uint64_t fit = (LDPC_STATIC_SCRATCH_BYTES - off_msgs) / (nw * per_slot);
+    const uint64_t grid = std::min<uint64_t>({(std::min<uint64_t>((uint64_t)n, kLaunchFrames) + nw - 1) / nw,
                                               (uint64_t)per_sm * n_sm, fit});
     unsigned int* d_work = reinterpret_cast<unsigned int*>(base);
     unsigned long long* d_tally = reinterpret_cast<unsigned long long*>(base + 64);
@@ -705,7 +716,10 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         snprintf(msg, sizeof msg, "static decode setup: %s", cudaGetErrorString(e));
         return sfail(LDPC_EIO, err, msg);
     }
-    if (grid > 0) {
+    for (uint64_t off = 0; e == cudaSuccess && grid > 0 && off < (uint64_t)n; off += kLaunchFrames) {
+        const uint64_t cnt = std::min<uint64_t>(kLaunchFrames, (uint64_t)n - off);
+        if (off) e = cudaMemsetAsync(d_work, 0, sizeof(unsigned int), stream);
+        if (e != cudaSuccess) break;
         GenParams gp;
         memset(&gp, 0, sizeof gp);
         gp.cols = d_cols;
@@ -719,19 +733,19 @@ int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const floa
         gp.l_max = p->l_max;
         gp.r_max = p->r_max;
         gp.l_post_max = p->l_post_max;
-        gp.n_frames = (uint32_t)n;
+        gp.n_frames = (uint32_t)cnt;
         gp.r_base = base + off_msgs;
-        gp.llr_in = d_llr;
-        gp.post_out = d_post;
-        gp.iters_out = d_iters;
-        gp.synd_out = d_synd;
-        gp.be_out = d_be;
+        gp.llr_in = d_llr + off * (uint64_t)(N - P);
+        gp.post_out = d_post ? d_post + off * (uint64_t)N : nullptr;
+        gp.iters_out = d_iters ? d_iters + off : nullptr;
+        gp.synd_out = d_synd ? d_synd + off : nullptr;
+        gp.be_out = d_be ? d_be + off : nullptr;
         gp.tally = d_tally;
         gp.hist = nullptr;
         gp.hist_bins = 1;
         gp.work = d_work;
         void* args[] = {&gp};
-        e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * GEN_WARPS), args, smem, stream);
+        e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(32 * nw), args, smem, stream);
     }
     unsigned long long t[TALLY_WORDS] = {};
     if (e == cudaSuccess) e = cudaMemcpyAsync(t, d_tally, sizeof t, cudaMemcpyDeviceToHost, stream);
