@@ -373,6 +373,20 @@ def measure_host_llr(dec, code, storage, frames: int = 1 << 16, repeats: int = 3
         return None
 
 
+def rank_totals(maxes, sums, dist=None, device=None):
+    """The multi-rank reduction of a bench line: the timings (device, end-to-end, wall seconds) as
+    the maximum over ranks, the counts (frames, iterations, launches, per-point tallies) summed; the
+    identity on one rank.  Every rank calls it once, in the same order."""
+    import torch
+    if dist is None:
+        return [float(x) for x in maxes], [float(x) for x in sums]
+    t = torch.tensor(list(maxes), dtype=torch.float64, device=device)
+    n = torch.tensor(list(sums), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return t.tolist(), n.tolist()
+
+
 def run_ours(args):
     import torch
 
@@ -397,12 +411,6 @@ def run_ours(args):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-
-    def allreduce(vals, op):
-        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(t, op=op)
-        return t.tolist()
 
     code = code_and_matrix()
     dec = capi.Decoder.from_code(code, local)
@@ -464,9 +472,9 @@ def run_ours(args):
     e2e_s = sum(a["e2e_s"] for a in acc.values())
     frames = sum(a["frames"] for a in acc.values())
     iters = sum(a["iters"] for a in acc.values())
-    maxes = allreduce([dev_s, e2e_s, wall], torch.distributed.ReduceOp.MAX if dist else None)
-    sums = allreduce([frames, iters, launches] + [acc[eb][k] for eb in POINTS for k in ("frames", "fe", "be", "iters")],
-                     torch.distributed.ReduceOp.SUM if dist else None)
+    maxes, sums = rank_totals([dev_s, e2e_s, wall],
+                              [frames, iters, launches] + [acc[eb][k] for eb in POINTS for k in ("frames", "fe", "be", "iters")],
+                              dist, "cuda")
     dev_max, e2e_max, wall_max = maxes
     tot_frames, tot_iters, tot_launches = sums[0], sums[1], sums[2]
     per_point_tot = {eb: dict(zip(("frames", "fe", "be", "iters"), sums[3 + 4 * k:7 + 4 * k])) for k, eb in enumerate(POINTS)}

@@ -10,7 +10,7 @@ on the identical sums, so every rank takes the same number of collective steps a
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import Callable, List, Sequence
+from typing import Callable, List, Sequence, Tuple
 
 TALLY_KEYS = ("frames", "bit_errors", "frame_errors", "iter_sum")
 
@@ -20,6 +20,18 @@ def frame_range(batch: int, world: int, rank: int, frames_per_rank: int):
     if not 0 <= rank < world:
         raise ValueError("rank outside the world")
     return (batch * world + rank) * frames_per_rank, frames_per_rank
+
+
+def split_range(first: int, n: int, parts: int) -> List[Tuple[int, int]]:
+    """The frames [first, first + n) in ``parts`` contiguous pieces (first, count), in order, sizes
+    differing by at most one; equal to ``frame_range`` of every rank when n = parts x F."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    out = []
+    for g in range(parts):
+        a, b = first + n * g // parts, first + n * (g + 1) // parts
+        out.append((a, b - a))
+    return out
 
 
 def allreduce_sum(values: Sequence[int], device=None) -> List[int]:

@@ -88,6 +88,7 @@ class Options:
     resume: str = ""
     circulant: str = ""
     damping: Optional[float] = None
+    gpus: int = 0  # 0: LDPC_SIM_GPUS from the environment, else 1
     extra: dict = field(default_factory=dict)
 
 
@@ -98,7 +99,8 @@ CIRC_MODES = {"device": (1, 1, 0.9375), "stepper": (0, 0, 1.0), "stepper-sfpi": 
 def parse_args(argv: List[str]) -> Options:
     o = Options()
     opts, _ = getopt.gnu_getopt(argv, "c:e:p:t:m:b:k:i:svnL:R:G:V:",
-                                ["storage=", "seed=", "device=", "out=", "resume=", "circulant=", "damping="])
+                                ["storage=", "seed=", "device=", "out=", "resume=", "circulant=", "damping=",
+                                 "gpus="])
     for k, v in opts:
         if k == "-c": o.matrix = v
         elif k == "-e": o.ebn0 = float(v)
@@ -128,6 +130,15 @@ def parse_args(argv: List[str]) -> Options:
                 raise getopt.GetoptError(f"--circulant must be one of {', '.join(CIRC_MODES)}, not {v}")
             o.circulant = v
         elif k == "--damping": o.damping = float(v)
+        elif k == "--gpus":
+            o.gpus = int(v)
+            if o.gpus < 1:
+                raise getopt.GetoptError("--gpus must be >= 1")
+    if o.gpus == 0:
+        env = os.environ.get("LDPC_SIM_GPUS", "")
+        o.gpus = int(env) if env.strip() else 1
+        if o.gpus < 1:
+            raise getopt.GetoptError("LDPC_SIM_GPUS must be >= 1")
     if o.damping is not None and not o.circulant:
         raise getopt.GetoptError("--damping needs --circulant")
     if o.circulant and (o.nms or o.l_max > 0 or o.r_max > 0 or o.l_post_max > 0 or o.gamma > 0):
@@ -194,6 +205,126 @@ class GpuEngine:
 TUNE_MIN_BLOCKS = 1 << 22  # runs at least this long pick their launch shape first
 
 
+class MultiGpuEngine:
+    """Several GPUs of one node in one process, one engine (device handle) and one host thread each:
+    every batch's frame range splits into contiguous pieces, piece g decoded on device g, and the
+    tallies are summed on the host once all have returned, as the reference's host sums its mesh
+    cores' stats after each batch (ldpc_sim_scalar.cpp:318-333,540-589).  The frames, and so the
+    tallies, are those of a one-GPU run of the same batches."""
+
+    def __init__(self, mat: chinn.Matrix, punctured: int, devices: List[int], factory: Callable):
+        from concurrent.futures import ThreadPoolExecutor
+        self.engines = []
+        try:
+            for d in devices:
+                self.engines.append(factory(mat, punctured, d))
+        except Exception:
+            self.close()
+            raise
+        self.pool = ThreadPoolExecutor(max_workers=len(self.engines))
+
+    def _all(self, fn):
+        return list(self.pool.map(fn, self.engines))
+
+    def describe(self) -> str:
+        return f"{self.engines[0].describe()} on {len(self.engines)} GPUs"
+
+    def set_circulant(self, o: Options):
+        self._all(lambda e: e.set_circulant(o))
+
+    def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
+        shapes = self._all(lambda e: e.tune(o, mu, sigma, max_blocks) if hasattr(e, "tune") else None)
+        return shapes[0]
+
+    def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
+        from .dist import split_range
+        pieces = split_range(first, n, len(self.engines))
+        rs = list(self.pool.map(lambda ep: ep[0].run(o, mu, sigma, l_max, ep[1][0], ep[1][1]),
+                                zip(self.engines, pieces)))
+        return Batch(sum(r.frames for r in rs), sum(r.bit_errors for r in rs), sum(r.frame_errors for r in rs),
+                     sum(r.iter_sum for r in rs), max(r.kernel_ms for r in rs))
+
+    def run_pair(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int):
+        """Lockstep verification across devices: the same frames on the first two GPUs."""
+        a, b = self.engines[0], self.engines[1]
+        f = [self.pool.submit(e.run, o, mu, sigma, l_max, first, n) for e in (a, b)]
+        return f[0].result(), f[1].result()
+
+    def close(self):
+        pool = getattr(self, "pool", None)
+        if pool:
+            pool.shutdown(wait=True)
+        for e in self.engines:
+            close = getattr(e, "close", None)
+            if close:
+                close()
+        self.engines = []
+
+
+class RankEngine:
+    """One rank of a torchrun job (one process per GPU): the rank's contiguous piece of every batch on
+    its own GPU, the four tallies summed over ranks by one all-reduce (torch.distributed: NCCL on
+    GPUs, gloo on CPU), so every rank sees the same sums, applies the same stop rule and takes the
+    same collective steps (ldpcb200.dist)."""
+
+    def __init__(self, inner, world: int, rank: int):
+        self.inner, self.world, self.rank = inner, world, rank
+
+    def describe(self) -> str:
+        return f"{self.inner.describe()}, rank {self.rank} of {self.world} processes"
+
+    def set_circulant(self, o: Options):
+        self.inner.set_circulant(o)
+
+    def tune(self, o: Options, mu: float, sigma: float, max_blocks: int):
+        return self.inner.tune(o, mu, sigma, max_blocks) if hasattr(self.inner, "tune") else None
+
+    def run(self, o: Options, mu: float, sigma: float, l_max: float, first: int, n: int) -> Batch:
+        from .dist import allreduce_sum, split_range
+        a, cnt = split_range(first, n, self.world)[self.rank]
+        r = self.inner.run(o, mu, sigma, l_max, a, cnt)
+        tot = allreduce_sum([r.frames, r.bit_errors, r.frame_errors, r.iter_sum], device=self.device())
+        return Batch(tot[0], tot[1], tot[2], tot[3], r.kernel_ms)
+
+    def device(self):
+        import torch.distributed as dist
+        return "cuda" if dist.get_backend() == "nccl" else None
+
+    def close(self):
+        close = getattr(self.inner, "close", None)
+        if close:
+            close()
+
+
+def _torchrun_world():
+    """(world, rank, local rank) when launched by torchrun, else None."""
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    if w <= 1:
+        return None
+    return w, int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _init_process_group() -> bool:
+    """Joins the torchrun job's process group unless the caller already did; True if this call
+    created it (and so destroys it at the end)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if dist.is_initialized():
+        return False
+    if torch.cuda.is_available():
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return True
+
+
+def _quiet(s: str):
+    pass
+
+
 def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = None, out=None) -> int:
     out = out or sys.stdout
     argv = sys.argv[1:] if argv is None else argv
@@ -207,6 +338,9 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
     except (getopt.GetoptError, ValueError) as e:
         print(f"ldpc_sim: {e}", file=sys.stderr)
         return 2
+    tr = _torchrun_world()
+    if tr and tr[1] != 0:  # under torchrun, rank 0 alone speaks the stdout protocol
+        say = _quiet
     try:
         path = resolve_filepath(o.matrix)
         mat = chinn.parse_chinn(path)
@@ -219,8 +353,17 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
     if not 0 <= o.punctured < mat.N:
         print(f"ldpc_sim: punctured count {o.punctured} outside [0, N)", file=sys.stderr)
         return 1
+    factory = engine_factory or GpuEngine
+    own_pg = False
     try:
-        engine = (engine_factory or GpuEngine)(mat, o.punctured, o.device)
+        if tr:  # torchrun: one process per GPU, this rank's piece of every batch
+            world, rank, local = tr
+            own_pg = _init_process_group()
+            engine = RankEngine(factory(mat, o.punctured, local), world, rank)
+        elif o.gpus > 1:  # one process, one host thread per GPU
+            engine = MultiGpuEngine(mat, o.punctured, list(range(o.device, o.device + o.gpus)), factory)
+        else:
+            engine = factory(mat, o.punctured, o.device)
     except Exception as e:  # no GPU, library missing, unsupported matrix: fail loudly
         print(f"ldpc_sim: cannot start the GPU engine: {e}", file=sys.stderr)
         return 1
@@ -235,7 +378,7 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
             return 1
     cores = 1 if o.single_core else MESH_CORES
     say(f"[CONFIG] Running in {'SINGLE-CORE' if o.single_core else 'MULTI-CORE'} accounting "
-        f"({cores} cores) on one GPU with the {engine.describe()}")
+        f"({cores} cores) with the {engine.describe()}")
     max_blocks = o.max_blocks
     if max_blocks == 0 and o.blocks_per_core > 0:
         max_blocks = o.blocks_per_core * cores
@@ -283,7 +426,7 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
             say(f"[CONFIG] Resuming at frame {blocks} from {o.resume}")
 
     csv = None
-    if o.out_csv:
+    if o.out_csv and say is not _quiet:
         exists = os.path.exists(o.out_csv)
         csv = open(o.out_csv, "a")
         if not exists:
@@ -308,8 +451,11 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
                 # independent launches and compared; the tallies count all cores' identical copies.
                 # The reference does not advance the generators in this mode: every batch repeats
                 # the same frames (:609-616), so every batch starts at frame 0 here too.
-                a = engine.run(o, mu, sigma, l_max, 0, cur)
-                b2 = engine.run(o, mu, sigma, l_max, 0, cur)
+                if isinstance(engine, MultiGpuEngine):  # the same frames on two GPUs
+                    a, b2 = engine.run_pair(o, mu, sigma, l_max, 0, cur)
+                else:
+                    a = engine.run(o, mu, sigma, l_max, 0, cur)
+                    b2 = engine.run(o, mu, sigma, l_max, 0, cur)
                 same = (a.bit_errors, a.frame_errors, a.iter_sum) == (b2.bit_errors, b2.frame_errors, b2.iter_sum)
                 if same:
                     say(f"[VERIFICATION PASS] All {cores} cores produced IDENTICAL output: bit_err={a.bit_errors}, "
@@ -334,11 +480,11 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
                 f"\"target_errors\": {o.target_fe}, \"ber\": {_g(ber)}, \"fer\": {_g(fer)}, "
                 f"\"throughput_msps\": {_g(msps)}, \"elapsed_sec\": {_g(el)}, "
                 f"\"mean_iters\": {_g(iters / blocks if blocks else 0.0)}, \"kernel_ms\": {_g(kernel_ms)}" + "}")
-            if csv:
+            if csv and say is not _quiet:
                 csv.write(f"{o.ebn0:.2f},{blocks},{be},{fe},{ber:.6e},{fer:.6e},"
                           f"{(iters / blocks if blocks else 0.0):.3f},{msps:.2f},{el:.2f}\n")
                 csv.flush()
-            if o.resume:
+            if o.resume and say is not _quiet:
                 tmp = o.resume + ".tmp"
                 with open(tmp, "w") as f:
                     json.dump({"matrix": path, "ebn0": o.ebn0, "seed": o.seed, "blocks": blocks,
@@ -353,6 +499,9 @@ def main(argv: Optional[List[str]] = None, engine_factory: Optional[Callable] = 
     el = time.perf_counter() - t0
     say("{" + f"\"ebn0\": {_g(o.ebn0)}, \"blocks\": {blocks}, \"bit_errors\": {be}, "
         f"\"frame_errors\": {fe}, \"elapsed_sec\": {_g(el)}" + "}")
+    if own_pg:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 
