@@ -338,18 +338,25 @@ def measured_peaks():
 
 
 def measure_host_llr(dec, code, storage, frames: int = 1 << 16, repeats: int = 3):
-    """Gsps of ldpc_decode_llr on frames whose channel LLRs sit in host memory, the host->device copy
-    of the LLRs and the device->host copy of the per-frame results inside the timing; LLRs from the
-    simulator's own channel at 2.5 dB.  The LLRs are in pinned host memory (the figure reported);
-    the same call from a pageable array is reported beside it."""
+    """Gsps of decoding caller LLRs from host memory (ldpc_decode_llr, ldpc_decode_llr_bf16), the
+    host->device copy of the LLRs and the device->host copy of the per-frame results inside the
+    timing; LLRs from the simulator's own channel at 2.5 dB.  `value`: bf16 LLRs (the reference's
+    channel storage, half the bytes) in page-locked memory; beside it the same from pageable memory
+    (staged through the library's pinned ring) and both for fp32 LLRs."""
     try:
+        import numpy as np
         import torch
         mu, sigma = mu_sigma(code, POINTS[0])
         p = dec.params(mu=mu, sigma=sigma, seed=SEED + 99, n_frames=frames, max_iter=MAX_ITER, storage=storage)
-        pageable = dec.channel_llr(p)
-        pinned_t = torch.empty(pageable.shape, dtype=torch.float32, pin_memory=True)
-        pinned = pinned_t.numpy()
-        pinned[...] = pageable
+        f32 = dec.channel_llr(p)
+        u = f32.view(np.uint32).astype(np.uint64)
+        b16 = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)  # bf16, round to nearest even
+
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.int16 if a.dtype == np.uint16 else torch.float32, pin_memory=True)
+            v = t.numpy().view(a.dtype)
+            v[...] = a
+            return v, t
 
         def best_time(llr):
             dec.decode_llr(llr, p, want_post=False)  # warm-up
@@ -361,13 +368,21 @@ def measure_host_llr(dec, code, storage, frames: int = 1 << 16, repeats: int = 3
                 best = dt if best is None else min(best, dt)
             return best
 
-        t_pin = best_time(pinned)
-        t_page = best_time(pageable)
-        return {"value": round(frames * code.n_tx / t_pin / 1e9, 4), "unit": UNIT, "frames": frames,
-                "h2d_bytes_per_step": int(pinned.nbytes), "d2h_bytes_per_step": int(frames * 12),
-                "pageable_value": round(frames * code.n_tx / t_page / 1e9, 4),
-                "path": "ldpc_decode_llr with host LLR arrays (pinned; pageable_value: the same from "
-                        "pageable memory), iterations, syndrome and bit-error counts back to the host"}
+        out = {}
+        for name, arr in (("bf16", b16), ("fp32", f32)):
+            pin, owner = pinned(arr)
+            out[name] = (best_time(pin), best_time(arr), int(arr.nbytes))
+            del pin, owner
+        g = lambda t: round(frames * code.n_tx / t / 1e9, 4)  # noqa: E731
+        return {"value": g(out["bf16"][0]), "unit": UNIT, "frames": frames,
+                "h2d_bytes_per_step": out["bf16"][2], "d2h_bytes_per_step": int(frames * 12),
+                "pageable_value": g(out["bf16"][1]),
+                "fp32_value": g(out["fp32"][0]), "fp32_pageable_value": g(out["fp32"][1]),
+                "fp32_h2d_bytes_per_step": out["fp32"][2],
+                "path": "ldpc_decode_llr_bf16 with host bf16 LLR arrays in page-locked memory (pageable_value: "
+                        "the same from pageable memory, staged through the library's pinned ring; fp32_*: "
+                        "ldpc_decode_llr with fp32 LLRs), iterations, syndrome and bit-error counts back to "
+                        "the host"}
     except Exception as e:  # an optional figure must not hide the GPU number
         log(f"host-LLR measurement failed: {e}")
         return None

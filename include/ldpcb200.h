@@ -141,6 +141,15 @@ int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, 
                     float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
                     ldpc_tally* out);
 
+/* As ldpc_decode_llr with the channel LLRs as bf16 values (the bit patterns, uint16 each), the form in
+ * which the reference's decoder holds its channel LLRs (ldpc_decoder_core.h:262-283): half the
+ * host->device bytes.  The values are widened to fp32 exactly on the device, so the results equal
+ * ldpc_decode_llr on the same values given as fp32.  A pageable array (either entry point) is
+ * staged through a ring of page-locked buffers that host threads fill while earlier pieces copy. */
+int ldpc_decode_llr_bf16(ldpc_handle* h, const ldpc_run_params* p, const uint16_t* llr, int64_t n_frames,
+                         float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
+                         ldpc_tally* out);
+
 /* Writes the channel LLRs the simulation would decode for frames first_frame .. +n_frames-1
  * (before storage rounding): llr [n_frames][N-P] (host).  For checking the channel. */
 int ldpc_channel_llr(ldpc_handle* h, const ldpc_run_params* p, float* llr);

@@ -6,10 +6,12 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ldpcb200.h"
@@ -101,6 +103,17 @@ struct ldpc_handle {
     // overlap the host->device copy of the next (created on first use)
     cudaStream_t cstream = nullptr;
     cudaEvent_t cev = nullptr;
+    // ldpc_decode_llr_bf16: the caller's bf16 LLRs on the device before they are widened
+    uint16_t* d_llr16 = nullptr;
+    size_t llr16_cap = 0;
+    // pageable caller arrays: a ring of pinned buffers the host fills while earlier pieces copy to the
+    // device (created on first use)
+    static constexpr int kStageSlots = 3;
+    static constexpr size_t kStageBytes = 32u << 20;
+    void* stage[kStageSlots] = {};
+    cudaEvent_t stage_ev[kStageSlots] = {};
+    bool stage_busy[kStageSlots] = {};
+    int stage_next = 0;
 };
 
 static int detect_qc(ldpc_handle* h) {
@@ -185,8 +198,14 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     if (h->h_tally) cudaFreeHost(h->h_tally);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->cev) cudaEventDestroy(h->cev);
     if (h->cstream) cudaStreamDestroy(h->cstream);
+    cudaFree(h->d_llr16);
+    for (int i = 0; i < ldpc_handle::kStageSlots; ++i) {
+        if (h->stage[i]) cudaFreeHost(h->stage[i]);
+        if (h->stage_ev[i]) cudaEventDestroy(h->stage_ev[i]);
+    }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -638,10 +657,143 @@ static int read_tally(ldpc_handle* h, ldpc_tally* out) {
 // Splits a request into launches of at most 2^31 frames (the kernel's claim counter is 32-bit).
 static constexpr uint64_t kMaxLaunchFrames = 1ull << 31;
 
-// h_llr (host, optional): the channel LLRs of the n frames, copied into d_llr one chunk at a time on
-// the handle's copy stream while the previous chunk decodes; chunk <= kMaxLaunchFrames.
+// Channel LLRs in host memory for ldpc_decode_llr / ldpc_decode_llr_bf16.
+struct HostLlr {
+    const void* src;  // [n][N-P] elements
+    int elem;         // 4: fp32; 2: bf16 bit patterns
+    bool pageable;    // not page-locked: staged through the pinned ring
+};
+
+// bf16 bit patterns -> fp32 (exact): eight values per thread and step when both arrays allow it.
+__global__ void widen_bf16_kernel(const uint16_t* __restrict__ in, float* __restrict__ out, uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const bool vec = (reinterpret_cast<uintptr_t>(in) % 16 == 0) && (reinterpret_cast<uintptr_t>(out) % 16 == 0);
+    uint64_t head = 0;
+    if (vec) {
+        const uint64_t n8 = n / 8;
+        for (uint64_t i = t; i < n8; i += stride) {
+            const uint4 v = reinterpret_cast<const uint4*>(in)[i];
+            float4 a, b;
+            a.x = __uint_as_float(v.x << 16); a.y = __uint_as_float(v.x & 0xFFFF0000u);
+            a.z = __uint_as_float(v.y << 16); a.w = __uint_as_float(v.y & 0xFFFF0000u);
+            b.x = __uint_as_float(v.z << 16); b.y = __uint_as_float(v.z & 0xFFFF0000u);
+            b.z = __uint_as_float(v.w << 16); b.w = __uint_as_float(v.w & 0xFFFF0000u);
+            reinterpret_cast<float4*>(out)[2 * i] = a;
+            reinterpret_cast<float4*>(out)[2 * i + 1] = b;
+        }
+        head = n8 * 8;
+    }
+    for (uint64_t i = head + t; i < n; i += stride) out[i] = __uint_as_float((uint32_t)in[i] << 16);
+}
+
+// Host copies on a pool of persistent threads (one per host thread, at most 16): the caller splits a
+// copy into equal parts, each worker takes one, the caller takes the first and waits for the rest.
+class CopyPool {
+  public:
+    static CopyPool& get() {
+        static CopyPool pool;
+        return pool;
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        constexpr size_t kMinPart = 1u << 20;
+        const size_t nt = std::min<size_t>(workers_.size() + 1, std::max<size_t>(1, bytes / kMinPart));
+        if (nt <= 1) {
+            memcpy(dst, src, bytes);
+            return;
+        }
+        std::lock_guard<std::mutex> serial(call_mu_);  // one copy at a time (handles on other threads wait)
+        const size_t part = (bytes / nt + 63) & ~(size_t)63;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = static_cast<char*>(dst);
+            src_ = static_cast<const char*>(src);
+            bytes_ = bytes;
+            part_ = part;
+            parts_ = nt;
+            pending_ = nt - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        memcpy(dst, src, std::min(bytes, part));
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+  private:
+    CopyPool() {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned n = std::min(16u, hw) - 1;
+        for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this, i] { run(i + 1); });
+    }
+    void run(size_t k) {
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            if (k >= parts_) continue;  // fewer parts than workers this time
+            char* d = dst_;
+            const char* s = src_;
+            const size_t a = std::min(bytes_, k * part_), b = std::min(bytes_, (k + 1) * part_);
+            lk.unlock();
+            if (a < b) memcpy(d + a, s + a, b - a);
+            lk.lock();
+            if (--pending_ == 0) done_cv_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_, call_mu_;
+    std::condition_variable cv_, done_cv_;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t bytes_ = 0, part_ = 0, parts_ = 0, pending_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+static void par_memcpy(void* dst, const void* src, size_t bytes) { CopyPool::get().copy(dst, src, bytes); }
+
+// Host -> device copy of `bytes` from a pageable array through the pinned ring, on the copy stream:
+// each piece waits for its slot's previous copy, is copied into the slot by host threads, then
+// copied to the device asynchronously, so the host fills one slot while others travel.
+static int stage_h2d(ldpc_handle* h, void* dst, const char* src, size_t bytes) {
+    for (int i = 0; i < ldpc_handle::kStageSlots; ++i) {
+        if (!h->stage[i] && cudaMallocHost(&h->stage[i], ldpc_handle::kStageBytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LDPC_ENOMEM, "pinned staging buffer allocation failed");
+        }
+        if (!h->stage_ev[i] && cudaEventCreateWithFlags(&h->stage_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return fail(LDPC_EIO, "staging event creation failed");
+    }
+    for (size_t done = 0; done < bytes;) {
+        const size_t piece = std::min(ldpc_handle::kStageBytes, bytes - done);
+        const int k = h->stage_next;
+        h->stage_next = (k + 1) % ldpc_handle::kStageSlots;
+        if (h->stage_busy[k]) CU(cudaEventSynchronize(h->stage_ev[k]));
+        par_memcpy(h->stage[k], src + done, piece);
+        CU(cudaMemcpyAsync(static_cast<char*>(dst) + done, h->stage[k], piece, cudaMemcpyHostToDevice, h->cstream));
+        CU(cudaEventRecord(h->stage_ev[k], h->cstream));
+        h->stage_busy[k] = true;
+        done += piece;
+    }
+    return 0;
+}
+
+// hin (optional): the channel LLRs of the n frames in host memory, copied into d_llr one chunk at a
+// time on the handle's copy stream (bf16 through d_llr16 and the widening kernel) while the
+// previous chunk decodes; chunk <= kMaxLaunchFrames.
 static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64_t n, const float* d_llr,
-                      float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be, const float* h_llr = nullptr,
+                      float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be, const HostLlr* hin = nullptr,
                       uint64_t chunk = kMaxLaunchFrames) {
     int rc;
     if ((rc = reset_counters(h))) return rc;
@@ -649,9 +801,22 @@ static int run_frames(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint64
     const uint64_t ntx = (uint64_t)(h->N - h->P);
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t cnt = (uint32_t)std::min<uint64_t>(chunk, n - off);
-        if (h_llr) {
-            CU(cudaMemcpyAsync(const_cast<float*>(d_llr) + off * ntx, h_llr + off * ntx, cnt * ntx * sizeof(float),
-                               cudaMemcpyHostToDevice, h->cstream));
+        if (hin) {
+            const size_t bytes = (size_t)cnt * ntx * hin->elem;
+            const char* src = static_cast<const char*>(hin->src) + off * ntx * hin->elem;
+            void* dst = hin->elem == 4 ? static_cast<void*>(const_cast<float*>(d_llr) + off * ntx)
+                                       : static_cast<void*>(h->d_llr16 + off * ntx);
+            if (hin->pageable) {
+                if ((rc = stage_h2d(h, dst, src, bytes))) return rc;
+            } else {
+                CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->cstream));
+            }
+            if (hin->elem == 2) {
+                widen_bf16_kernel<<<h->n_sm * 4, 256, 0, h->cstream>>>(h->d_llr16 + off * ntx,
+                                                                       const_cast<float*>(d_llr) + off * ntx,
+                                                                       (uint64_t)cnt * ntx);
+                CU(cudaGetLastError());
+            }
             CU(cudaEventRecord(h->cev, h->cstream));
             CU(cudaStreamWaitEvent(h->stream, h->cev, 0));
         }
@@ -703,9 +868,9 @@ extern "C" int ldpc_run_chunk(ldpc_handle* h, const ldpc_run_params* p, ldpc_tal
     return read_tally(h, out);
 }
 
-extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, int64_t n,
-                               float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
-                               ldpc_tally* out) {
+// ldpc_decode_llr and ldpc_decode_llr_bf16: caller LLRs of `elem` bytes each (4: fp32, 2: bf16).
+static int decode_host(ldpc_handle* h, const ldpc_run_params* p, const void* llr, int elem, int64_t n, float* post,
+                       int32_t* iters, int32_t* synd_fail, int32_t* bit_errors, ldpc_tally* out) {
     int rc;
     if ((rc = check_params(h, p))) return rc;
     if (n < 0) return fail(LDPC_EINVAL, "n_frames < 0");
@@ -715,23 +880,31 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
     const size_t nb = (size_t)n;
     if (nb) {
         if ((rc = ensure_cap((void**)&h->d_llr, &h->llr_cap, nb * ntx * sizeof(float)))) return rc;
+        if (elem == 2 && (rc = ensure_cap((void**)&h->d_llr16, &h->llr16_cap, nb * ntx * sizeof(uint16_t))))
+            return rc;
         if (post && (rc = ensure_cap((void**)&h->d_post, &h->post_cap, nb * h->N * sizeof(float)))) return rc;
         if ((rc = ensure_cap((void**)&h->d_frame_out, &h->frame_cap, 3 * nb * sizeof(int32_t)))) return rc;
     }
-    // Large calls copy the LLRs in chunks on a second stream, so that the decoding of one chunk
-    // overlaps the copy of the next; small ones copy everything first.
-    constexpr uint64_t kMinChunk = 8192;
-    const bool pipelined = nb >= 2 * kMinChunk;
-    uint64_t chunk = kMaxLaunchFrames;
-    if (pipelined) {
-        if (!h->cstream && cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) != cudaSuccess)
-            return fail(LDPC_EIO, "copy stream creation failed");
-        if (!h->cev && cudaEventCreateWithFlags(&h->cev, cudaEventDisableTiming) != cudaSuccess)
-            return fail(LDPC_EIO, "copy event creation failed");
-        chunk = std::min<uint64_t>(kMaxLaunchFrames, std::max<uint64_t>(kMinChunk, (nb + 7) / 8));
-    } else if (nb) {
-        CU(cudaMemcpyAsync(h->d_llr, llr, nb * ntx * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    if (!h->cstream && cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(LDPC_EIO, "copy stream creation failed");
+    if (!h->cev && cudaEventCreateWithFlags(&h->cev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(LDPC_EIO, "copy event creation failed");
+    // A page-locked array is copied by DMA straight from the caller's memory; a pageable one through
+    // the handle's pinned ring, filled by host threads.
+    bool pageable = true;
+    if (nb) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, llr) == cudaSuccess)
+            pageable = a.type == cudaMemoryTypeUnregistered;
+        else
+            cudaGetLastError();
     }
+    // Large calls copy the LLRs in chunks on the copy stream, so that the decoding of one chunk
+    // overlaps the copy of the next; small ones are one chunk.
+    constexpr uint64_t kMinChunk = 8192;
+    uint64_t chunk = kMaxLaunchFrames;
+    if (nb >= 2 * kMinChunk) chunk = std::min<uint64_t>(kMaxLaunchFrames, std::max<uint64_t>(kMinChunk, (nb + 7) / 8));
+    const HostLlr hin{llr, elem, pageable};
     ldpc_run_params q = *p;
     q.first_frame = 0;
     q.n_frames = nb;
@@ -739,7 +912,7 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
     int32_t* d_sf = d_it ? d_it + nb : nullptr;
     int32_t* d_be = d_sf ? d_sf + nb : nullptr;
     if ((rc = run_frames(h, &q, true, nb, h->d_llr, post ? h->d_post : nullptr, d_it, d_sf, d_be,
-                         pipelined ? llr : nullptr, chunk)))
+                         nb ? &hin : nullptr, chunk)))
         return rc;
     if (nb) {
         if (post) CU(cudaMemcpyAsync(post, h->d_post, nb * h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -748,6 +921,18 @@ extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const f
         if (bit_errors) CU(cudaMemcpyAsync(bit_errors, d_be, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     }
     return read_tally(h, out);
+}
+
+extern "C" int ldpc_decode_llr(ldpc_handle* h, const ldpc_run_params* p, const float* llr, int64_t n,
+                               float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
+                               ldpc_tally* out) {
+    return decode_host(h, p, llr, 4, n, post, iters, synd_fail, bit_errors, out);
+}
+
+extern "C" int ldpc_decode_llr_bf16(ldpc_handle* h, const ldpc_run_params* p, const uint16_t* llr, int64_t n,
+                                    float* post, int32_t* iters, int32_t* synd_fail, int32_t* bit_errors,
+                                    ldpc_tally* out) {
+    return decode_host(h, p, llr, 2, n, post, iters, synd_fail, bit_errors, out);
 }
 
 // Channel only: the Philox/Box-Muller LLRs of a range of frames, for checking the generator.

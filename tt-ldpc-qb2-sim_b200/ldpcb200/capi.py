@@ -24,6 +24,7 @@ STORAGE_NAMES = {"bf16": STORE_BF16, "fp32": STORE_FP32, "fp16": STORE_FP16}
 
 # The entry points include/ldpcb200.h declares (tests check that the library exports each one).
 EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", "ldpc_decode_llr",
+           "ldpc_decode_llr_bf16",
            "ldpc_channel_llr", "ldpc_channel_llr_device", "ldpc_iter_histogram", "ldpc_snr_bins",
            "ldpc_set_launch_shape", "ldpc_list_shapes", "ldpc_list_shapes_algo", "ldpc_set_weights",
            "ldpc_set_circulant",
@@ -99,6 +100,8 @@ def load(path: str = LIB_PATH):
     L.ldpc_run_chunk.argtypes = [C.c_void_p, P(RunParams), P(Tally)]
     L.ldpc_decode_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), C.c_int64, P(C.c_float),
                                   P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
+    L.ldpc_decode_llr_bf16.argtypes = [C.c_void_p, P(RunParams), P(C.c_uint16), C.c_int64, P(C.c_float),
+                                       P(C.c_int32), P(C.c_int32), P(C.c_int32), P(Tally)]
     L.ldpc_channel_llr.argtypes = [C.c_void_p, P(RunParams), P(C.c_float)]
     L.ldpc_iter_histogram.argtypes = [C.c_void_p, P(C.c_uint64), C.c_int]
     L.ldpc_snr_bins.argtypes = [C.c_void_p, P(C.c_uint64)]
@@ -320,11 +323,13 @@ class Decoder:
                            t.max_iters, t.kernel_ms, t.bit_errors_sq)
 
     def decode_llr(self, llr: np.ndarray, p: Optional[RunParams] = None, want_post: bool = True, **kw):
-        """Decode caller-supplied channel LLRs [n, N-P].  Returns (post [n, N] or None, iters,
-        synd_fail, bit_errors, ChunkResult)."""
+        """Decode caller-supplied channel LLRs [n, N-P]: fp32, or uint16 arrays holding bf16 bit
+        patterns (ldpc_decode_llr_bf16).  Returns (post [n, N] or None, iters, synd_fail, bit_errors,
+        ChunkResult)."""
         if p is None:
             p = self.params(**kw)
-        llr = np.ascontiguousarray(np.atleast_2d(llr), dtype=np.float32)
+        bf16 = isinstance(llr, np.ndarray) and llr.dtype == np.uint16
+        llr = np.ascontiguousarray(np.atleast_2d(llr), dtype=np.uint16 if bf16 else np.float32)
         if llr.shape[1] != self.n_tx:
             raise ValueError(f"llr has {llr.shape[1]} columns, expected N-P = {self.n_tx}")
         n = llr.shape[0]
@@ -333,8 +338,12 @@ class Decoder:
         sf = np.empty(n, np.int32)
         be = np.empty(n, np.int32)
         t = Tally()
-        _check(self._lib.ldpc_decode_llr(self._h, C.byref(p), _fp(llr), n, _fp(post), _ip(it), _ip(sf),
-                                         _ip(be), C.byref(t)))
+        if bf16:
+            _check(self._lib.ldpc_decode_llr_bf16(self._h, C.byref(p), llr.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                                  n, _fp(post), _ip(it), _ip(sf), _ip(be), C.byref(t)))
+        else:
+            _check(self._lib.ldpc_decode_llr(self._h, C.byref(p), _fp(llr), n, _fp(post), _ip(it), _ip(sf),
+                                             _ip(be), C.byref(t)))
         return post, it, sf, be, ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum,
                                              t.unconverged, t.max_iters, t.kernel_ms, t.bit_errors_sq)
 
