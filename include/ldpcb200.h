@@ -308,6 +308,12 @@ void ldpc_batch_destroy(ldpc_batch* b);
 int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, const float* share, ldpc_tally* out,
                    float* graph_ms);
 
+/* How many times the batch built and instantiated its CUDA graph.  The graph is built by the first
+ * ldpc_batch_run and relaunched by later ones with its kernel nodes updated in place (arguments,
+ * kernel, grid, shared memory: other frame counts, storage modes, shapes or shares); a call that
+ * changes which codes have frames rebuilds it. */
+int64_t ldpc_batch_graph_builds(const ldpc_batch* b);
+
 /* Copies the last error message of the calling thread into buf (NUL-terminated); returns its
  * length. */
 int ldpc_last_error(char* buf, size_t len);

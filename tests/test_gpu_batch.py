@@ -75,3 +75,36 @@ def test_mixed_workload_small(gpu):
             assert r.frame_errors <= r.frames * 0.5  # every Eb/N0 is at least 0.5 dB above threshold
     finally:
         w.close()
+
+
+def test_graph_built_once_and_relaunched(gpu):
+    """Repeated calls relaunch the batch's one instantiated graph with its kernel nodes updated (other
+    frame counts and so grids, seeds, frame ranges, another storage mode and so another kernel) and
+    tally what separate runs tally; a call that leaves a code without frames rebuilds the graph."""
+    codes = [ar4ja.make_code(K, r) for K, r in CODES]
+    decs = [capi.Decoder.from_code(c, 0) for c in codes]
+    try:
+        b = capi.Batch(decs)
+        for rep, counts in enumerate(([600, 200, 40], [900, 100, 60], [300, 300, 20])):
+            ps = [_params(d, c, i, n) for i, (c, d, n) in enumerate(zip(codes, decs, counts))]
+            for p in ps:
+                p.seed = 100 + rep
+                p.first_frame += 7777 * rep
+            res, _ = b.run(ps)
+            assert b.graph_builds == 1
+            for i, (d, p) in enumerate(zip(decs, ps)):
+                s = d.run_chunk(p)
+                assert (res[i].frames, res[i].bit_errors, res[i].frame_errors, res[i].iter_sum) == \
+                    (s.frames, s.bit_errors, s.frame_errors, s.iter_sum)
+        ps = [_params(d, c, i, n, storage="fp16" if i == 0 else "bf16")
+              for i, (c, d, n) in enumerate(zip(codes, decs, [500, 50, 10]))]
+        res, _ = b.run(ps)
+        s0 = decs[0].run_chunk(ps[0])
+        assert b.graph_builds == 1 and res[0].frames == 500 and res[0].iter_sum == s0.iter_sum
+        ps[1].n_frames = 0
+        res, _ = b.run(ps)
+        assert b.graph_builds == 2 and res[1].frames == 0 and res[2].frames == 10
+        b.close()
+    finally:
+        for d in decs:
+            d.close()

@@ -376,8 +376,11 @@ void free_general(GeneralCode* g) {
     cudaFree(g->d_r);
     cudaFree(g->d_scols[0]);
     cudaFree(g->d_scols[1]);
+    cudaFree(g->d_slot[0]);
+    cudaFree(g->d_slot[1]);
     g->d_cols = g->d_runs = nullptr;
     g->d_scols[0] = g->d_scols[1] = nullptr;
+    g->d_slot[0] = g->d_slot[1] = nullptr;
     g->d_r = nullptr;
     g->r_cap = 0;
     g->sdt = 0;

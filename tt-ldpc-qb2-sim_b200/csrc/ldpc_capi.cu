@@ -1029,13 +1029,23 @@ extern "C" int ldpc_snr_bins(ldpc_handle* h, uint64_t* out) {
 // ----------------------------------------------------------------------------- batched launch
 // Several codes decoded by one CUDA graph launch: per code, memset nodes for its counters followed by
 // its persistent kernel; the codes' kernels have no dependencies on one another and run side by
-// side, each on its share of the GPU's CTA slots, each claiming frames from its own queue.
+// side, each on its share of the GPU's CTA slots, each claiming frames from its own queue.  The graph
+// is built and instantiated once and relaunched: a call updates its kernel nodes in place
+// (cudaGraphExecKernelNodeSetParams: arguments, kernel, grid and shared-memory size may all change),
+// and rebuilds the graph only when the set of codes with frames changes (a code's kernel node
+// appears or goes) or an update is refused.
+
 struct ldpc_batch {
     int device = 0;
     std::vector<ldpc_handle*> hs;
     cudaStream_t stream = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int64_t launches = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char> key;                // per code: 1 if it has a kernel node
+    std::vector<cudaGraphNode_t> knode;   // per code, its kernel node in `graph`
+    int64_t builds = 0;
 };
 
 extern "C" int ldpc_batch_create(ldpc_handle* const* handles, int n, ldpc_batch** out) {
@@ -1065,11 +1075,15 @@ extern "C" void ldpc_batch_destroy(ldpc_batch* b) {
     if (!b) return;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
+
+extern "C" int64_t ldpc_batch_graph_builds(const ldpc_batch* b) { return b ? b->builds : -1; }
 
 static int add_memset(cudaGraph_t g, void* dst, size_t bytes, cudaGraphNode_t* node) {
     cudaMemsetParams mp = {};
@@ -1098,56 +1112,88 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
         if (!(w[i] >= 0.0)) return fail(LDPC_EINVAL, "share %d is negative", i);
         work_total += params[i].n_frames ? w[i] : 0.0;
     }
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t ge = nullptr;
-    CU(cudaGraphCreate(&g, 0));
+    // every code's launch first (prepare_qc may grow a code's message scratch, so its arguments
+    // change from call to call even when nothing else does)
+    std::vector<QcLaunch> Ls(n);
+    std::vector<char> key(n, 0);
     int rc = 0;
     int64_t kernels = 0;
-    for (int i = 0; i < n && !rc; ++i) {
-        ldpc_handle* h = b->hs[i];
-        cudaGraphNode_t deps[4];
-        if ((rc = add_memset(g, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), &deps[0])) ||
-            (rc = add_memset(g, h->d_work, 64, &deps[1])) ||
-            (rc = add_memset(g, h->d_hist, h->hist_bins * sizeof(unsigned long long), &deps[2])) ||
-            (rc = add_memset(g, h->d_snr, 4 * SNR_BINS * sizeof(unsigned long long), &deps[3])))
-            break;
+    for (int i = 0; i < n; ++i) {
         if (!params[i].n_frames) continue;
-        QcLaunch L;
         // no shares: every kernel gets its full persistent grid and the block scheduler starts the
         // next code's CTAs as the previous code's retire
         const double frac = (share && work_total > 0.0) ? w[i] / work_total : 1.0;
-        rc = prepare_qc(h, &params[i], false, (uint32_t)params[i].n_frames, params[i].first_frame, nullptr, nullptr,
-                        nullptr, nullptr, nullptr, frac, &L);
-        if (rc == LDPC_ENOTSUP) {
-            rc = fail(LDPC_ENOTSUP, "code %d: no QC kernel for these options", i);
-            break;
-        }
-        if (rc || !L.grid) continue;
-        void* args[] = {&L.qp};
-        cudaKernelNodeParams kp = {};
-        kp.func = const_cast<void*>(L.fn);
-        kp.gridDim = dim3(L.grid);
-        kp.blockDim = dim3(L.block);
-        kp.sharedMemBytes = (unsigned)L.smem;
-        kp.kernelParams = args;
-        cudaGraphNode_t kn;
-        const cudaError_t e = cudaGraphAddKernelNode(&kn, g, deps, 4, &kp);
-        if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphAddKernelNode: %s", cudaGetErrorString(e));
+        rc = prepare_qc(b->hs[i], &params[i], false, (uint32_t)params[i].n_frames, params[i].first_frame, nullptr,
+                        nullptr, nullptr, nullptr, nullptr, frac, &Ls[i]);
+        if (rc == LDPC_ENOTSUP) return fail(LDPC_ENOTSUP, "code %d: no QC kernel for these options", i);
+        if (rc) return rc;
+        if (!Ls[i].grid) continue;
+        key[i] = 1;
         ++kernels;
     }
-    if (!rc) {
-        const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-        if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    auto kparams = [&](int i, void** args) {
+        cudaKernelNodeParams kp = {};
+        kp.func = const_cast<void*>(Ls[i].fn);
+        kp.gridDim = dim3(Ls[i].grid);
+        kp.blockDim = dim3(Ls[i].block);
+        kp.sharedMemBytes = (unsigned)Ls[i].smem;
+        kp.kernelParams = args;
+        return kp;
+    };
+    bool reuse = b->exec && b->key.size() == key.size() && std::equal(key.begin(), key.end(), b->key.begin());
+    if (reuse) {
+        for (int i = 0; i < n && reuse; ++i) {
+            if (!key[i]) continue;
+            void* args[] = {&Ls[i].qp};
+            const cudaKernelNodeParams kp = kparams(i, args);
+            if (cudaGraphExecKernelNodeSetParams(b->exec, b->knode[i], &kp) != cudaSuccess) {
+                cudaGetLastError();
+                reuse = false;  // rebuild below
+            }
+        }
     }
-    if (!rc) {
+    if (!reuse) {
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->graph) cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+        b->key.clear();
+        b->knode.assign(n, nullptr);
+        cudaGraph_t g = nullptr;
+        CU(cudaGraphCreate(&g, 0));
+        b->graph = g;
+        for (int i = 0; i < n && !rc; ++i) {
+            ldpc_handle* h = b->hs[i];
+            cudaGraphNode_t deps[4];
+            if ((rc = add_memset(g, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), &deps[0])) ||
+                (rc = add_memset(g, h->d_work, 64, &deps[1])) ||
+                (rc = add_memset(g, h->d_hist, h->hist_bins * sizeof(unsigned long long), &deps[2])) ||
+                (rc = add_memset(g, h->d_snr, 4 * SNR_BINS * sizeof(unsigned long long), &deps[3])))
+                break;
+            if (!key[i]) continue;
+            void* args[] = {&Ls[i].qp};
+            const cudaKernelNodeParams kp = kparams(i, args);
+            const cudaError_t e = cudaGraphAddKernelNode(&b->knode[i], g, deps, 4, &kp);
+            if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphAddKernelNode: %s", cudaGetErrorString(e));
+        }
+        if (!rc) {
+            const cudaError_t e = cudaGraphInstantiate(&b->exec, g, 0);
+            if (e != cudaSuccess) {
+                b->exec = nullptr;
+                rc = fail(LDPC_EIO, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+            }
+        }
+        if (rc) return rc;
+        b->key = key;
+        ++b->builds;
+    }
+    {
         cudaError_t e = cudaEventRecord(b->e0, b->stream);
-        if (e == cudaSuccess) e = cudaGraphLaunch(ge, b->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, b->stream);
         if (e == cudaSuccess) e = cudaEventRecord(b->e1, b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) rc = fail(LDPC_EIO, "graph launch: %s", cudaGetErrorString(e));
     }
-    if (ge) cudaGraphExecDestroy(ge);
-    if (g) cudaGraphDestroy(g);
     if (rc) return rc;
     b->launches += kernels;
     float ms = 0.0f;

@@ -37,6 +37,7 @@ struct GeneralCode {
     // without a row and an edge past its row's degree point at the dummy posterior slot N
     int sdt = 0;                          // its degree bound (0: the matrix needs the warp kernel)
     int32_t* d_scols[2] = {nullptr, nullptr};  // byte offsets for 2- and 4-byte posteriors, step_table layout
+    int32_t* d_slot[2] = {nullptr, nullptr};   // [N] the shared-memory slot of each variable, per element size
     int step_ctas = 0;                    // step kernel CTAs per SM (0: as many as fit)
 };
 
@@ -61,6 +62,7 @@ struct GenParams {
     float ebn0_lo, ebn0_hi, rate;         // per-frame Eb/N0 (see QcParams)
     unsigned long long* snr_bins;
     const int32_t* scols;                 // step kernel: its column table (byte offsets)
+    const int32_t* slot;                  // step kernel: [N] shared-memory slot of each variable
     int32_t n_steps;
 };
 

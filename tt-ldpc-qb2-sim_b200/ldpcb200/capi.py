@@ -30,6 +30,7 @@ EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", 
            "ldpc_set_circulant",
            "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
+           "ldpc_batch_graph_builds",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_row_schedule", "ldpc_last_error",
            "ldpc_abi_version")
 
@@ -109,6 +110,8 @@ def load(path: str = LIB_PATH):
     L.ldpc_batch_destroy.argtypes = [C.c_void_p]
     L.ldpc_batch_destroy.restype = None
     L.ldpc_batch_run.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), P(Tally), P(C.c_float)]
+    L.ldpc_batch_graph_builds.argtypes = [C.c_void_p]
+    L.ldpc_batch_graph_builds.restype = C.c_int64
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_list_shapes_algo.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int32), C.c_int]
@@ -406,6 +409,11 @@ class Batch:
         res = [ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
                            t.kernel_ms, t.bit_errors_sq) for t in T]
         return res, ms.value
+
+    @property
+    def graph_builds(self) -> int:
+        """How many times the batch built its CUDA graph (once, unless a call changed a kernel)."""
+        return int(self._lib.ldpc_batch_graph_builds(self._b))
 
     def close(self):
         if getattr(self, "_b", None):
