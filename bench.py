@@ -828,6 +828,8 @@ def mixed_measure(wl, total, warmup, steps, world=1, rank=0, warm_frames=None, c
             res, ms = step(i, total)
             out["e2e_s"] += time.perf_counter() - t0
             out["dev_ms"] += ms
+            if i == 0:
+                out["first_ms"] = ms
             for c, r in zip(wl.codes, res):
                 out["frames"] += r.frames
                 out["symbols"] += r.frames * r.n_tx
@@ -873,8 +875,17 @@ def mixed_subrecord(args, local):
     try:
         m = mixed_measure(wl, args.mixed_frames, 3, 2, warm_frames=1 << 20, clock_gpus=(local,))
         dev_s = m["dev_ms"] / 1e3
+        # the first timed launch's frames again, each code alone on the whole GPU, after the timing
+        alone = wl.run_alone(args.mixed_frames, seed=SEED, first_frame=0)
         return {
+            "codes_alone": {"ms": {c.name: round(t, 2) for c, t in zip(wl.codes, alone)},
+                            "sum_ms": round(sum(alone), 2),
+                            "graph_ms_over_sum": round(m["first_ms"] / max(sum(alone), 1e-9), 4),
+                            "what": "the first timed launch's frames, each code's share in a launch of its own "
+                                    "(same frames, per-frame Eb/N0, storage, shape); graph_ms_over_sum < 1 means "
+                                    "running the nine kernels side by side in one graph beats running them in turn"},
             "workload": MIXED_WORKLOAD, "frames_per_launch": args.mixed_frames, "steps": 2, "warmup": 3,
+            "order": wl.order,
             "value": round(m["symbols"] / dev_s / 1e9, 4), "unit": UNIT,
             "frames_per_s": round(m["frames"] / dev_s, 1), "graph_ms_per_launch": round(m["dev_ms"] / 2, 2),
             "e2e": {"value": round(m["symbols"] / m["e2e_s"] / 1e9, 4), "unit": UNIT,

@@ -299,14 +299,29 @@ int ldpc_batch_create(ldpc_handle* const* handles, int n_handles, ldpc_batch** o
 void ldpc_batch_destroy(ldpc_batch* b);
 
 /* One graph launch: per handle i, params[i] (n_frames may be 0; at most 2^31) decoded by its
- * persistent kernel.  The kernels have no dependencies on one another.  With share NULL each gets its
- * full persistent grid and the hardware block scheduler starts a code's CTAs as the CTAs launched
- * before it retire; otherwise kernel i is limited to the fraction share[i] / sum(share) of the
- * GPU's CTA slots and the codes run side by side.
+ * persistent kernel, in the order ldpc_batch_set_order chose.  With share NULL each kernel gets its
+ * full persistent grid (kernels without a dependency between them: the hardware block scheduler
+ * starts a code's CTAs as the CTAs launched before it retire); otherwise kernel i is limited to the
+ * fraction share[i] / sum(share) of the GPU's CTA slots.
  * out[i] receives handle i's tallies (kernel_ms = the whole graph's device time), *graph_ms the
  * device time of the launch.  ldpc_snr_bins(handle i) then gives its per-Eb/N0 tallies. */
 int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, const float* share, ldpc_tally* out,
                    float* graph_ms);
+
+/* Order of the batch's kernels inside its graph:
+ *   LDPC_BATCH_SIDE_BY_SIDE  no dependencies between the kernels (the block scheduler interleaves
+ *                            their CTAs as resources free up);
+ *   LDPC_BATCH_IN_TURN       each code's kernel starts when the previous code's has finished, so every
+ *                            kernel has the GPU (and its L2) to itself;
+ *   LDPC_BATCH_GLOBAL_IN_TURN  the kernels that keep their check messages in global memory (the
+ *                            K = 16384 codes and the register-capped degree-18 shapes, whose message
+ *                            scratch lives in L2) run in turn, the others side by side with them.
+ * A change of order rebuilds the graph at the next ldpc_batch_run.  Default: LDPC_BATCH_IN_TURN (on the
+ * nine-code workload it equals the sum of each code's kernel run alone, and is the steadiest). */
+#define LDPC_BATCH_SIDE_BY_SIDE 0
+#define LDPC_BATCH_IN_TURN 1
+#define LDPC_BATCH_GLOBAL_IN_TURN 2
+int ldpc_batch_set_order(ldpc_batch* b, int order);
 
 /* How many times the batch built and instantiated its CUDA graph.  The graph is built by the first
  * ldpc_batch_run and relaunched by later ones with its kernel nodes updated in place (arguments,

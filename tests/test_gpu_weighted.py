@@ -242,22 +242,39 @@ def _synd_fail(code, post):
     return par.sum(-1)
 
 
+_ORACLE_MODE = {"fp32": oracle.STORE_FP32, "fp16": oracle.STORE_FP16, "bf16": oracle.STORE_BF16}
+
+
 @pytest.mark.parametrize("K,rate,storages", [(1024, "1/2", ("fp32", "fp16", "bf16")), (4096, "4/5", ("fp16", "bf16"))])
-def test_weighted_sim_kernel_at_unit_weights_is_the_plain_kernel(gpu, K, rate, storages):
+@pytest.mark.parametrize("granularity", ["edge", "check"])
+def test_weighted_sim_kernel_at_unit_weights_is_the_plain_kernel(gpu, K, rate, storages, granularity):
+    """Unit weights: the plain decoder's values.  The weighted decoder tests the syndrome from the
+    first iteration, the plain one (the reference's rule) from the third: a frame that stops at
+    iteration 1 or 2 holds the oracle's posteriors after that many iterations and satisfies every
+    check; every other frame stops where the plain decoder stops, with its bits."""
     code = ar4ja.make_code(K, rate)
     llr = _llr(code, 40, 2.0 if rate == "1/2" else 3.2, 41)
+    nc = weighted.n_classes(code, granularity)
+    oc = oracle.Code(code.row_matrix(), code.N, code.P)
     with capi.Decoder.from_code(code, 0) as dec:
-        dec.set_weights(np.ones((4, code.n_classes)), np.zeros((4, code.n_classes)), weighted.edge_class_table(code))
+        dec.set_weights(np.ones((4, nc)), np.zeros((4, nc)), weighted.edge_class_table(code, granularity))
         for st in storages:
             a = dec.decode_llr(llr, max_iter=30, storage=st, algo=capi.ALGO_AMIN)
             w = dec.decode_llr(llr, max_iter=30, storage=st, algo=capi.ALGO_WAMIN)
-            assert np.array_equal(a[0].view(np.uint32), w[0].view(np.uint32)), st
+            late = w[1] >= 3
+            assert late.any(), st
+            assert np.array_equal(a[0][late].view(np.uint32), w[0][late].view(np.uint32)), st
             for x, y in zip(a[1:4], w[1:4]):
-                assert np.array_equal(x, y), st
+                assert np.array_equal(x[late], y[late]), st
+            for f in np.flatnonzero(~late):
+                assert w[2][f] == 0 and a[1][f] >= 3, (st, f)
+                po, _, _, _ = oracle.decode(oc, llr[f:f + 1], mode=_ORACLE_MODE[st], max_iter=int(w[1][f]),
+                                            early_stop=False)
+                assert np.array_equal(w[0][f].view(np.uint32), po[0].view(np.uint32)), (st, f)
 
 
 def test_weighted_sim_kernel_matches_torch_reference_with_early_stop(gpu):
-    """fp32 messages, trained-like weights: every frame stops at the first iteration >= 3 whose hard
+    """fp32 messages, trained-like weights: every frame stops at the first iteration whose hard
     decisions satisfy all checks (or at max_iter), and its posterior is the reference's after that
     many iterations, bit for bit."""
     code = ar4ja.make_code(1024, "1/2")
@@ -270,7 +287,7 @@ def test_weighted_sim_kernel_matches_torch_reference_with_early_stop(gpu):
     ref = wref.decode(code, torch.from_numpy(llr), a, b).numpy()  # [T][n][N]
     fails = np.stack([_synd_fail(code, ref[t]) for t in range(T)])  # [T][n]
     for f in range(llr.shape[0]):
-        stop = next((t + 1 for t in range(2, T) if fails[t, f] == 0), T)
+        stop = next((t + 1 for t in range(T) if fails[t, f] == 0), T)
         assert it[f] == stop, (f, it[f], stop)
         assert np.array_equal(post[f].view(np.uint32), ref[stop - 1, f].view(np.uint32)), f
         assert sf[f] == fails[stop - 1, f]
@@ -352,3 +369,65 @@ def test_weighted_offset_table_shapes_equal_default(gpu, K, rate, storage):
             dec.set_launch_shape(0, 0, 0, 0, storage=storage)
             for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters", "bit_errors_sq"):
                 assert getattr(r, k) == getattr(base, k), (sh, k)
+
+
+def _row_uniform_params(code, T, seed):
+    """Random (alpha, beta) per iteration and protograph check row, as a check-granularity table and
+    as the same values spread over the per-edge classes."""
+    g = np.random.default_rng(seed)
+    ar = (0.7 + 0.6 * g.random((T, 3))).astype(np.float32)
+    br = (-0.2 + 0.4 * g.random((T, 3))).astype(np.float32)
+    ae = np.zeros((T, code.n_classes), np.float32)
+    be = np.zeros((T, code.n_classes), np.float32)
+    for l, cls in enumerate(code.edge_class):
+        ae[:, cls] = ar[:, [l // 4]]
+        be[:, cls] = br[:, [l // 4]]
+    return (ar, br), (ae, be)
+
+
+@pytest.mark.parametrize("K,rate,storage,shape", [(1024, "1/2", "fp32", None), (1024, "1/2", "fp32", (1, 1, 5, 2)),
+                                                  (1024, "1/2", "fp16", (1, 1, 6, 2)), (1024, "1/2", "bf16", None),
+                                                  (4096, "4/5", "fp16", (1, 1, 0, 2)), (4096, "4/5", "bf16", (1, 1, 8, 1)),
+                                                  (4096, "4/5", "fp32", (1, 1, 8, 1))])
+def test_row_weights_equal_per_edge_weights(gpu, K, rate, storage, shape):
+    """Weights with one class per protograph check row run on the per-row kernels (the pair applied
+    to the row's two magnitudes); the same values given per edge run on the per-edge kernels.  The two
+    decode the same frames to the same bits, iterations and tallies, through the simulation kernel
+    and through caller LLRs."""
+    code = ar4ja.make_code(K, rate)
+    T = 15
+    (ar, br), (ae, be) = _row_uniform_params(code, T, 7)
+    llr = _llr(code, 64, 1.8 if rate == "1/2" else 3.0, 17)
+    mu, sigma = capi.channel_mu_sigma(code.N, code.n_checks, code.P, 1.8 if rate == "1/2" else 3.0)
+    out = []
+    for a, b, gran in ((ar, br, "check"), (ae, be, "edge")):
+        with capi.Decoder.from_code(code, 0) as dec:
+            dec.set_weights(a, b, weighted.edge_class_table(code, gran))
+            if shape:
+                dec.set_launch_shape(*shape, storage=storage)
+            d = dec.decode_llr(llr, max_iter=T, storage=storage, algo=capi.ALGO_WAMIN)
+            r = dec.run_chunk(dec.params(mu=mu, sigma=sigma, seed=5, n_frames=3000, max_iter=T, storage=storage,
+                                         algo=capi.ALGO_WAMIN))
+            out.append((d, r))
+    (d0, r0), (d1, r1) = out
+    assert np.array_equal(d0[0].view(np.uint32), d1[0].view(np.uint32))
+    for x, y in zip(d0[1:4], d1[1:4]):
+        assert np.array_equal(x, y)
+    assert (r0.frames, r0.bit_errors, r0.frame_errors, r0.iter_sum, r0.max_iters) == \
+        (r1.frames, r1.bit_errors, r1.frame_errors, r1.iter_sum, r1.max_iters)
+    assert r0.frames == 3000 and r0.iter_sum > 3000
+
+
+def test_row_weights_list_the_per_row_shapes(gpu):
+    """A check-granularity table makes the per-row kernels the handle's weighted shapes; the
+    autotuner times them like any other shape."""
+    code = ar4ja.make_code(1024, "1/2")
+    (ar, br), _ = _row_uniform_params(code, 10, 3)
+    with capi.Decoder.from_code(code, 0) as dec:
+        edge_shapes = dec.shapes("fp32", capi.ALGO_WAMIN)
+        dec.set_weights(ar, br, weighted.edge_class_table(code, "check"))
+        assert set(dec.shapes("fp32", capi.ALGO_WAMIN)) == set(edge_shapes)
+        mu, sigma = capi.channel_mu_sigma(code.N, code.n_checks, code.P, 2.5)
+        res, best = dec.autotune(mu, sigma, storages=("fp32",), frames=1 << 14, max_iter=20, algo=capi.ALGO_WAMIN,
+                                 repeats=1)
+        assert best == "fp32" and res["fp32"][0] in edge_shapes

@@ -95,6 +95,10 @@ struct ldpc_handle {
     // weights of LDPC_ALGO_WAMIN runs
     float2* d_wtab = nullptr;  // [w_iters][w_slots] (alpha, beta) per iteration and edge slot
     int w_iters = 0, w_slots = 0;
+    // when every row's edges share one class: [w_iters][12] (alpha, beta) per iteration and layer,
+    // for the per-row weighted kernels (ALGO_WROW)
+    float2* d_wtab_row = nullptr;
+    bool w_row = false;
     // settings of LDPC_ALGO_CIRC runs (default: the circulant engine on silicon)
     ldpc_circ_config circ{LDPC_CIRC_SFPU, LDPC_CIRC_STOP_GENIE, 0.9375f, 0};
     unsigned long long* h_tally = nullptr;  // pinned
@@ -194,6 +198,7 @@ extern "C" void ldpc_destroy(ldpc_handle* h) {
     cudaFree(h->d_frame_out);
     cudaFree(h->d_rmsg);
     cudaFree(h->d_wtab);
+    cudaFree(h->d_wtab_row);
     free_general(&h->gen);
     if (h->h_tally) cudaFreeHost(h->h_tally);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -326,11 +331,17 @@ static bool default_shape(const ldpc_handle* h, int storage, int algo, int clip,
     return false;
 }
 
+static bool default_shape_exists(const ldpc_handle* h, int storage, int algo) {
+    int s[4];
+    return default_shape(h, storage, algo, 0, 0, s);
+}
+
 extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float* beta, int n_iter, int n_classes,
                                 const int32_t* edge_class) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     if (n_iter == 0) {
         h->w_iters = 0;
+        h->w_row = false;
         return 0;
     }
     if (h->kind != LDPC_KERNEL_QC) return fail(LDPC_ENOTSUP, "the weighted decoder needs a QC code");
@@ -356,13 +367,36 @@ extern "C" int ldpc_set_weights(ldpc_handle* h, const float* alpha, const float*
                 tab[(size_t)t * slots + qc_edge_slot(l, e, h->D)] = make_float2(alpha[k], beta[k]);
             }
     CU(cudaSetDevice(h->device));
+    // one class per row (every edge of a layer in the same class): also the per-layer table of the
+    // per-row kernels
+    bool row_uniform = true;
+    for (int l = 0; l < QC_LAYERS; ++l)
+        for (int e = 1; e < (l < 4 ? QC_DEG_LOW : h->D); ++e)
+            row_uniform = row_uniform && edge_class[l * QC_DMAX + e] == edge_class[l * QC_DMAX];
+    std::vector<float2> tab_row;
+    if (row_uniform) {
+        tab_row.resize((size_t)n_iter * QC_LAYERS);
+        for (int t = 0; t < n_iter; ++t)
+            for (int l = 0; l < QC_LAYERS; ++l) {
+                const size_t k = (size_t)t * n_classes + edge_class[l * QC_DMAX];
+                tab_row[(size_t)t * QC_LAYERS + l] = make_float2(alpha[k], beta[k]);
+            }
+    }
     cudaFree(h->d_wtab);
+    cudaFree(h->d_wtab_row);
     h->d_wtab = nullptr;
+    h->d_wtab_row = nullptr;
     h->w_iters = 0;
+    h->w_row = false;
     CU(cudaMalloc(&h->d_wtab, cnt * sizeof(float2)));
     CU(cudaMemcpy(h->d_wtab, tab.data(), cnt * sizeof(float2), cudaMemcpyHostToDevice));
+    if (row_uniform) {
+        CU(cudaMalloc(&h->d_wtab_row, tab_row.size() * sizeof(float2)));
+        CU(cudaMemcpy(h->d_wtab_row, tab_row.data(), tab_row.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    }
     h->w_iters = n_iter;
     h->w_slots = slots;
+    h->w_row = row_uniform;
     return 0;
 }
 
@@ -408,6 +442,7 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
     bool any = reset;
     auto built = [&](int s) {
         return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G) ||
+               find_shape(h, s, ALGO_WROW, 0, 0, R, F, B, G) ||
                find_shape(h, s, LDPC_ALGO_CIRC, 0, 0, R, F, B, G);
     };
     for (int s = lo; s <= hi; ++s) any |= built(s);
@@ -442,6 +477,8 @@ extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo
         for (int i = 0; i < n && i < max_shapes; ++i) std::copy(list[i], list[i] + 4, shapes + 4 * i);
         return n;
     }
+    // weights with one class per row: the per-row weighted kernels' shapes, where any are built
+    if (algo == LDPC_ALGO_WAMIN && h->w_row && default_shape_exists(h, storage, ALGO_WROW)) algo = ALGO_WROW;
     for (const QcTable* t = qc_tables(); t; t = t->next)
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
@@ -504,16 +541,26 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
                       const float* d_llr, float* d_post, int32_t* d_it, int32_t* d_sf, int32_t* d_be,
                       double grid_frac, QcLaunch* out) {
     const bool clip = p->l_max > 0.0f || p->r_max > 0.0f || p->l_post_max > 0.0f;
-    int sh[4] = {h->shape[p->storage][0], h->shape[p->storage][1], h->shape[p->storage][2], h->shape[p->storage][3]};
-    const void* fn = nullptr;
-    if (sh[0] || sh[1] || sh[2] || sh[3])
-        fn = find_shape(h, p->storage, p->algo, clip, ext, sh[0] ? sh[0] : 1, sh[1] ? sh[1] : 1, sh[2], sh[3]);
-    if (fn) {
-        sh[0] = sh[0] ? sh[0] : 1;
-        sh[1] = sh[1] ? sh[1] : 1;
-    } else if (default_shape(h, p->storage, p->algo, clip, ext, sh)) {
-        fn = find_shape(h, p->storage, p->algo, clip, ext, sh[0], sh[1], sh[2], sh[3]);
-    }
+    int sh[4];
+    // the handle's shape for this storage, else the default shape of the algorithm
+    auto lookup = [&](int algo) -> const void* {
+        int s[4] = {h->shape[p->storage][0], h->shape[p->storage][1], h->shape[p->storage][2],
+                    h->shape[p->storage][3]};
+        const void* f = nullptr;
+        if (s[0] || s[1] || s[2] || s[3])
+            f = find_shape(h, p->storage, algo, clip, ext, s[0] ? s[0] : 1, s[1] ? s[1] : 1, s[2], s[3]);
+        if (f) {
+            s[0] = s[0] ? s[0] : 1;
+            s[1] = s[1] ? s[1] : 1;
+        } else if (default_shape(h, p->storage, algo, clip, ext, s)) {
+            f = find_shape(h, p->storage, algo, clip, ext, s[0], s[1], s[2], s[3]);
+        }
+        if (f) std::copy(s, s + 4, sh);
+        return f;
+    };
+    // weights with one class per row run on the per-row weighted kernels where they are built
+    const bool wrow = p->algo == LDPC_ALGO_WAMIN && h->w_row && lookup(ALGO_WROW);
+    const void* fn = lookup(wrow ? ALGO_WROW : p->algo);
     if (!fn) return LDPC_ENOTSUP;  // the caller falls back to the general kernel
     const int R = sh[0], F = sh[1], G = sh[3];
     QcParams& qp = out->qp;
@@ -547,9 +594,9 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     qp.rate = (float)code_rate(h);
     qp.snr_bins = h->d_snr;
     if (p->algo == LDPC_ALGO_WAMIN) {
-        qp.wtab = h->d_wtab;
+        qp.wtab = wrow ? h->d_wtab_row : h->d_wtab;
         qp.w_iters = h->w_iters;
-        qp.w_slots = h->w_slots;
+        qp.w_slots = wrow ? QC_LAYERS : h->w_slots;
     }
     if (p->algo == LDPC_ALGO_CIRC) {
         // the engine's edge order is ascending column: inside a layer every edge has its own column
@@ -593,7 +640,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     size_t smem = (size_t)F * lstride * esz + (size_t)F * (h->N / 32) * 4;
     if (G == 2 || p->algo == LDPC_ALGO_WAMIN) smem = (smem + 15) & ~(size_t)15;
     if (G == 2) smem += (size_t)T * (QC_DEG_LOW * 4 + h->D * 8) * 4;
-    if (p->algo == LDPC_ALGO_WAMIN) smem += (size_t)h->w_iters * h->w_slots * sizeof(float2);
+    if (p->algo == LDPC_ALGO_WAMIN) smem += (size_t)qp.w_iters * qp.w_slots * sizeof(float2);
     if (smem > 48 * 1024) CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
@@ -1046,6 +1093,8 @@ struct ldpc_batch {
     std::vector<char> key;                // per code: 1 if it has a kernel node
     std::vector<cudaGraphNode_t> knode;   // per code, its kernel node in `graph`
     int64_t builds = 0;
+    int order = LDPC_BATCH_IN_TURN;         // LDPC_BATCH_*: dependencies between the kernel nodes
+    int built_order = -1;                   // the order `graph` was built with
 };
 
 extern "C" int ldpc_batch_create(ldpc_handle* const* handles, int n, ldpc_batch** out) {
@@ -1084,6 +1133,14 @@ extern "C" void ldpc_batch_destroy(ldpc_batch* b) {
 }
 
 extern "C" int64_t ldpc_batch_graph_builds(const ldpc_batch* b) { return b ? b->builds : -1; }
+
+extern "C" int ldpc_batch_set_order(ldpc_batch* b, int order) {
+    if (!b) return fail(LDPC_EINVAL, "batch is NULL");
+    if (order < LDPC_BATCH_SIDE_BY_SIDE || order > LDPC_BATCH_GLOBAL_IN_TURN)
+        return fail(LDPC_EINVAL, "unknown batch order %d", order);
+    b->order = order;
+    return 0;
+}
 
 static int add_memset(cudaGraph_t g, void* dst, size_t bytes, cudaGraphNode_t* node) {
     cudaMemsetParams mp = {};
@@ -1140,7 +1197,14 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
         kp.kernelParams = args;
         return kp;
     };
-    bool reuse = b->exec && b->key.size() == key.size() && std::equal(key.begin(), key.end(), b->key.begin());
+    // the kernels chained one after another (LDPC_BATCH_IN_TURN: all of them; GLOBAL_IN_TURN: those
+    // with a message scratch in global memory); the chain's membership is part of the graph's shape
+    for (int i = 0; i < n; ++i)
+        if (key[i] && (b->order == LDPC_BATCH_IN_TURN ||
+                       (b->order == LDPC_BATCH_GLOBAL_IN_TURN && Ls[i].qp.r_base != nullptr)))
+            key[i] = 2;
+    bool reuse = b->exec && b->built_order == b->order && b->key.size() == key.size() &&
+                 std::equal(key.begin(), key.end(), b->key.begin());
     if (reuse) {
         for (int i = 0; i < n && reuse; ++i) {
             if (!key[i]) continue;
@@ -1162,19 +1226,23 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
         cudaGraph_t g = nullptr;
         CU(cudaGraphCreate(&g, 0));
         b->graph = g;
+        cudaGraphNode_t chain = nullptr;  // the last chained kernel node
         for (int i = 0; i < n && !rc; ++i) {
             ldpc_handle* h = b->hs[i];
-            cudaGraphNode_t deps[4];
+            cudaGraphNode_t deps[5];
             if ((rc = add_memset(g, h->d_tally, TALLY_WORDS * sizeof(unsigned long long), &deps[0])) ||
                 (rc = add_memset(g, h->d_work, 64, &deps[1])) ||
                 (rc = add_memset(g, h->d_hist, h->hist_bins * sizeof(unsigned long long), &deps[2])) ||
                 (rc = add_memset(g, h->d_snr, 4 * SNR_BINS * sizeof(unsigned long long), &deps[3])))
                 break;
             if (!key[i]) continue;
+            int nd = 4;
+            if (key[i] == 2 && chain) deps[nd++] = chain;
             void* args[] = {&Ls[i].qp};
             const cudaKernelNodeParams kp = kparams(i, args);
-            const cudaError_t e = cudaGraphAddKernelNode(&b->knode[i], g, deps, 4, &kp);
+            const cudaError_t e = cudaGraphAddKernelNode(&b->knode[i], g, deps, nd, &kp);
             if (e != cudaSuccess) rc = fail(LDPC_EIO, "cudaGraphAddKernelNode: %s", cudaGetErrorString(e));
+            if (key[i] == 2) chain = b->knode[i];
         }
         if (!rc) {
             const cudaError_t e = cudaGraphInstantiate(&b->exec, g, 0);
@@ -1185,6 +1253,7 @@ extern "C" int ldpc_batch_run(ldpc_batch* b, const ldpc_run_params* params, cons
         }
         if (rc) return rc;
         b->key = key;
+        b->built_order = b->order;
         ++b->builds;
     }
     {

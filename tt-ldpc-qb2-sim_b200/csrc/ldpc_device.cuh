@@ -18,7 +18,12 @@
 namespace ldpcb200 {
 
 enum Storage : int { STORE_BF16 = 0, STORE_FP32 = 1, STORE_FP16 = 2 };
-enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2, ALGO_CIRC = 3 };
+// ALGO_WROW is not a separate decoder: it is the weighted decoder (ALGO_WAMIN) for weight tables whose
+// classes are uniform over each row's edges (one (alpha, beta) per protograph check row), which the
+// kernels apply once per row instead of once per edge.  Callers request ALGO_WAMIN; the library
+// picks the per-row kernel when the table allows it.
+enum Algo : int { ALGO_AMIN = 0, ALGO_NMS = 1, ALGO_WAMIN = 2, ALGO_CIRC = 3, ALGO_WROW = 4 };
+constexpr bool algo_weighted(int a) { return a == ALGO_WAMIN || a == ALGO_WROW; }
 
 // ------------------------------------------------------------------ Philox-4x32-10
 struct U32x4 { uint32_t x, y, z, w; };

@@ -61,7 +61,8 @@ struct QcParams {
     unsigned long long* snr_bins;         // [4][SNR_BINS]: frames, frame errors, bit errors, iterations
     // weighted Approximate-Min* (ALGO_WAMIN): check output sign * max(alpha * m - beta, 0)
     // (alpha, beta) per iteration and edge slot: [w_iters][w_slots], edge e of layer l at slot
-    // qc_edge_slot(l, e, D); iteration t uses row min(t, w_iters - 1)
+    // qc_edge_slot(l, e, D); iteration t uses row min(t, w_iters - 1).  ALGO_WROW: one pair per
+    // iteration and layer, [w_iters][12].  Both test the syndrome from the first iteration on.
     const float2* wtab;
     int32_t w_iters, w_slots;
     // ALGO_CIRC stop rule and tally (the circulant engine's): QC_STOP_SYNDROME tests the syndrome
@@ -180,7 +181,10 @@ template <int d, int MODE> struct RowMsgGlobal {
 // Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
 // sL + f*lstride).  idx[e]: the row's column indices.
 // ALGO_WAMIN: wt[f] points at the (alpha, beta) pairs of this layer's edges for slot f's current
-// iteration (edge e at wt[f][e]: a constant offset, no class lookup).
+// iteration (edge e at wt[f][e]: a constant offset, no class lookup).  ALGO_WROW: wt[f][0] is the
+// layer's one pair, applied to the row's two magnitudes before they are spread over the edges (the
+// same values as ALGO_WAMIN with that pair on every edge, at two multiplies per row instead of one
+// per edge).
 // BO: idx[e] holds byte offsets into the slot's L array instead of element indices (the column
 // offset table of the OT layout), so no index scaling is needed.
 // PAD: rows of a smaller degree padded to d with edges whose posterior is the largest finite value
@@ -217,7 +221,7 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         // (9999 for Approximate-Min*, 999 for min-sum), the first minimum winning.
         bool is_am[d];
         float mag_min, mag_all;
-        if (ALGO == ALGO_AMIN || ALGO == ALGO_WAMIN) {
+        if (ALGO == ALGO_AMIN || algo_weighted(ALGO)) {
             // Prefix minima pm_i = min(9999, |q_0|, .., |q_i|); mn = pm_{d-1}.  The argmin index am is
             // the first i with |q_i| = mn, so i < am exactly when pm_i > mn: no index is tracked.
             // The other edges in row order are o_i = |q_i| for i < am and |q_{i+1}| after it, and the
@@ -233,9 +237,9 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
             for (int i = 0; i < d; ++i) lt[i] = (i + 1 < d) ? (pm[i] > mn) : false;
 #pragma unroll
             for (int e = 0; e < d; ++e) is_am[e] = (e == 0 ? true : lt[e - 1]) && !lt[e];
-            float m = lt[0] ? a[0] : a[1];
+            float m = fabsf(lt[0] ? q[f][0] : q[f][1]);
 #pragma unroll
-            for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, lt[i] ? a[i] : a[i + 1]);
+            for (int i = 1; i + 1 < d; ++i) m = amin_step_fma(m, fabsf(lt[i] ? q[f][i] : q[f][i + 1]));
             if (PAD) m = m > 1e38f ? mn : m;
             mag_min = m;
             mag_all = amin_step_fma(m, mn);
@@ -258,6 +262,13 @@ __device__ __forceinline__ void row_update(const int (&idx)[d], typename LTraits
         if (CLIP) {
             mag_min = fminf(mag_min, r_cap);
             mag_all = fminf(mag_all, r_cap);
+        }
+        if (ALGO == ALGO_WROW) {  // max(alpha * m - beta, 0) once per row
+            const float2 w = wt[f][0];
+            const float zmin = __fsub_rn(__fmul_rn(w.x, mag_min), w.y);
+            const float zall = __fsub_rn(__fmul_rn(w.x, mag_all), w.y);
+            mag_min = zmin > 0.0f ? zmin : 0.0f;
+            mag_all = zall > 0.0f ? zall : 0.0f;
         }
         // r_e = +-mag with sign parity ^ sign(q_e): fold the parity into the magnitudes once.
         const uint32_t smin = __float_as_uint(mag_min) | par;
@@ -600,7 +611,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                     (uint32_t)((p.blk_off[l][e] + ((tid + p.shift[l][e]) & (Z - 1))) * (int)sizeof(LE));
         }
     }
-    if constexpr (ALGO == ALGO_WAMIN) {  // visible after the first refill's barrier
+    if constexpr (algo_weighted(ALGO)) {  // visible after the first refill's barrier
         for (int i = tid; i < p.w_iters * p.w_slots; i += T) sW[i] = p.wtab[i];
     }
 
@@ -691,15 +702,17 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             const float2* wt[F];
 #pragma unroll
             for (int f = 0; f < F; ++f)
-                wt[f] = ALGO == ALGO_WAMIN ? sW + min(it[f], p.w_iters - 1) * p.w_slots : nullptr;
+                wt[f] = algo_weighted(ALGO) ? sW + min(it[f], p.w_iters - 1) * p.w_slots : nullptr;
             // OT: each layer's offsets are loaded one layer ahead, so their shared-memory latency
-            // overlaps the previous row update.  ALGO_CIRC visits the degree-D layers first (the
+            // overlaps the previous row update; two register sets take the layers in turn (no copy
+            // between them: +1.5 % on r1/2 K=1024 fp32 against copying the next set into the
+            // current one).  ALGO_CIRC visits the degree-D layers first (the
             // circulant engine's tile schedule, rows 512..1535 before 0..511 for K = 1024:
             // engines/circulant_dma_4cw/ar4ja_circulant_descriptors_4cw.h:29-31).
-            int pre[OT ? D : 1];
+            int offs[2][OT ? D : 1];
             if constexpr (OT) {
-                if constexpr (CIRC) ot_load<D, T>(sOT + T * ot_layer_start(4, D), tid, pre);
-                else ot_load<QC_DEG_LOW, T>(sOT, tid, pre);
+                if constexpr (CIRC) ot_load<D, T>(sOT + T * ot_layer_start(4, D), tid, offs[0]);
+                else ot_load<QC_DEG_LOW, T>(sOT, tid, offs[0]);
             }
 #pragma unroll
             for (int l = 0; l < QC_LAYERS; ++l) {
@@ -707,14 +720,14 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 const int ly_next = CIRC ? (l + 5) % QC_LAYERS : l + 1;
                 const float2* wl[F];
 #pragma unroll
-                for (int f = 0; f < F; ++f) wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(ly, 0, D) : nullptr;
-                int cur[OT ? D : 1];
-                if constexpr (OT) {  // this layer's offsets; start loading the next layer's
-#pragma unroll
-                    for (int e = 0; e < D; ++e) cur[e] = pre[e];
+                for (int f = 0; f < F; ++f)
+                    wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(ly, 0, D) : (ALGO == ALGO_WROW ? wt[f] + ly : nullptr);
+                int (&cur)[OT ? D : 1] = offs[l & 1];  // this layer's offsets
+                if constexpr (OT) {                     // start loading the next layer's
                     if (l + 1 < QC_LAYERS) {
-                        if (ly_next < 4) ot_load<QC_DEG_LOW, T>(sOT + T * ot_layer_start(ly_next, D), tid, pre);
-                        else ot_load<D, T>(sOT + T * ot_layer_start(ly_next, D), tid, pre);
+                        const uint32_t* nt = sOT + T * ot_layer_start(ly_next, D);
+                        if (ly_next < 4) ot_load<QC_DEG_LOW, T>(nt, tid, offs[(l + 1) & 1]);
+                        else ot_load<D, T>(nt, tid, offs[(l + 1) & 1]);
                     }
                 }
 #pragma unroll
@@ -780,11 +793,15 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
         }
 
         // ---------------------------------------------------------------- syndrome / stop
+        // The reference engine tests the syndrome from the third iteration on
+        // (ldpc_decoder_core.h:524-526); the circulant engine and the weighted decoder (no
+        // counterpart in the reference) from the first.
+        constexpr int stop_from = (CIRC || algo_weighted(ALGO)) ? 1 : 3;
         uint32_t eval = 0;
 #pragma unroll
         for (int f = 0; f < F; ++f)
             if ((act >> f) & 1u)
-                if (it[f] >= (CIRC ? 1 : 3) || it[f] >= p.max_iter) eval |= 1u << f;
+                if (it[f] >= stop_from || it[f] >= p.max_iter) eval |= 1u << f;
         if (!eval) continue;
         {
             // Pre-check: the sign parity of each thread's own rows in the two layers updated first in
@@ -878,7 +895,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
             if constexpr (CIRC)
                 conv = it[f] >= 1 && (p.stop_rule == QC_STOP_GENIE ? s_be[f] == 0 : s_sfail[f] == 0);
             else
-                conv = it[f] >= 3 && s_sfail[f] == 0;
+                conv = it[f] >= stop_from && s_sfail[f] == 0;
             if (conv) stopped |= 1u << f;
             if (conv || it[f] >= p.max_iter) done |= 1u << f;
         }

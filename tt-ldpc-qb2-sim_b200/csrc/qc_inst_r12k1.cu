@@ -66,5 +66,20 @@ static const QcEntry qc_r12k1[] = {
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_WAMIN, false, false, 5),
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_WAMIN, false, false, 6),
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_WAMIN, false, true, 0),
+    // the same shapes with one (alpha, beta) per row (weights of one class per protograph check row)
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, false),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_WROW, false, false),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, false, 5),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, false, 6),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, false, 8),
+    LDPC_QC_ENTRY_B(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, false, 5),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, true),
+    LDPC_QC_ENTRY(128, 6, 1, 1, STORE_BF16, ALGO_WROW, false, true),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, false, 0),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, false, 5),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_WROW, false, false, 6),
+    LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_WROW, false, true, 0),
 };
 LDPC_QC_REGISTER(qc_r12k1)

@@ -27,6 +27,13 @@ static const QcEntry qc_r45k4[] = {
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_BF16, ALGO_WAMIN, false, false, 0),
+    // the same shapes with one (alpha, beta) per row (weights of one class per protograph check row)
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_FP16, ALGO_WROW, false, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_WROW, false, false),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_FP16, ALGO_WROW, false, true),
+    LDPC_QC_ENTRY(128, 18, 1, 1, STORE_BF16, ALGO_WROW, false, true),
+    LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_FP16, ALGO_WROW, false, false, 0),
+    LDPC_QC_ENTRY_OT(128, 18, 1, 1, STORE_BF16, ALGO_WROW, false, false, 0),
     // check messages in global memory (layout 1): the 156 per-thread message registers of the
     // register layout leave room for only 8-10 warps per SM; without them the kernel holds more frames
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
@@ -36,5 +43,14 @@ static const QcEntry qc_r45k4[] = {
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 8),
+    // the weighted decoders in the same layout (per-edge and per-row weights)
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_WAMIN, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_WAMIN, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_WAMIN, false, true, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_WROW, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_WROW, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_WROW, false, false, 8),
+    LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_WROW, false, true, 8),
 };
 LDPC_QC_REGISTER(qc_r45k4)

@@ -30,7 +30,7 @@ EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", 
            "ldpc_set_circulant",
            "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
-           "ldpc_batch_graph_builds",
+           "ldpc_batch_graph_builds", "ldpc_batch_set_order",
            "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_row_schedule", "ldpc_last_error",
            "ldpc_abi_version")
 
@@ -112,6 +112,7 @@ def load(path: str = LIB_PATH):
     L.ldpc_batch_run.argtypes = [C.c_void_p, P(RunParams), P(C.c_float), P(Tally), P(C.c_float)]
     L.ldpc_batch_graph_builds.argtypes = [C.c_void_p]
     L.ldpc_batch_graph_builds.restype = C.c_int64
+    L.ldpc_batch_set_order.argtypes = [C.c_void_p, C.c_int]
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_list_shapes_algo.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int32), C.c_int]
@@ -385,9 +386,13 @@ class Decoder:
         return h
 
 
+BATCH_SIDE_BY_SIDE, BATCH_IN_TURN, BATCH_GLOBAL_IN_TURN = 0, 1, 2
+BATCH_ORDERS = {"side-by-side": BATCH_SIDE_BY_SIDE, "in-turn": BATCH_IN_TURN, "global-in-turn": BATCH_GLOBAL_IN_TURN}
+
+
 class Batch:
-    """Several decoders (codes) on one GPU run by one CUDA graph launch, their persistent kernels side
-    by side (ldpc_batch_* in include/ldpcb200.h)."""
+    """Several decoders (codes) on one GPU run by one CUDA graph launch of their persistent kernels
+    (ldpc_batch_* in include/ldpcb200.h); ``order`` says which kernels wait for one another."""
 
     def __init__(self, decoders):
         self._lib = load()
@@ -409,6 +414,12 @@ class Batch:
         res = [ChunkResult(t.frames, t.bit_errors, t.frame_errors, t.iter_sum, t.unconverged, t.max_iters,
                            t.kernel_ms, t.bit_errors_sq) for t in T]
         return res, ms.value
+
+    def set_order(self, order):
+        """BATCH_SIDE_BY_SIDE, BATCH_IN_TURN or BATCH_GLOBAL_IN_TURN (or its name)."""
+        if isinstance(order, str):
+            order = BATCH_ORDERS[order]
+        _check(self._lib.ldpc_batch_set_order(self._b, int(order)))
 
     @property
     def graph_builds(self) -> int:

@@ -15,6 +15,7 @@ else from the T = 20 file extended (iterations past the trained ones reuse the l
 iteration's weights).
 
     python -m ldpcb200.compare [--codes 1024:1/2 4096:4/5] [--ebn0 2.0 2.5 3.0] [--frames N]
+                               [--tags "" check_stop]
 """
 from __future__ import annotations
 
@@ -33,13 +34,13 @@ SEED = 0xC0DE5
 PLAIN_ITERS = 200
 
 
-def _weights_for(code: ar4ja.QcCode, cap: int, override: Optional[str] = None) -> Tuple[dict, str]:
+def _weights_for(code: ar4ja.QcCode, cap: int, override: Optional[str] = None, tag: str = "") -> Tuple[dict, str]:
     if override:
         return weighted.load_weights(override), os.path.basename(override)
-    exact = weighted.weights_path(code, cap)
+    exact = weighted.weights_path(code, cap, tag)
     if os.path.exists(exact):
         return weighted.load_weights(exact), os.path.basename(exact)
-    base = weighted.weights_path(code, 20)
+    base = weighted.weights_path(code, 20, tag)
     if not os.path.exists(base):
         raise FileNotFoundError(f"no trained weights for {code.name}: {base}")
     return weighted.load_weights(base), os.path.basename(base) + f" extended to {cap}"
@@ -53,7 +54,7 @@ def _tune(dec: capi.Decoder, code: ar4ja.QcCode, ebn0: float, max_iter: int, alg
 
 def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps: Sequence[int],
                  time_frames: int, device: int = 0, log=print, min_errors: int = 1000,
-                 weights: Optional[str] = None, controls: bool = True) -> dict:
+                 weights: Optional[str] = None, controls: bool = True, tags: Sequence[str] = ("",)) -> dict:
     decs: List[capi.Decoder] = []
     names: List[str] = []
     iters: List[int] = []
@@ -68,13 +69,14 @@ def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps:
         decs.append(plain); names.append(f"plain_{PLAIN_ITERS}"); iters.append(PLAIN_ITERS)
         algos.append(capi.ALGO_AMIN); storages.append(st)
         for cap in caps:
-            d = capi.Decoder.from_code(code, device)
-            w, src = _weights_for(code, cap, weights)
-            weighted.apply_weights(d, code, w, cap)
-            st, _ = _tune(d, code, mid, cap, capi.ALGO_WAMIN, tune_frames)
-            decs.append(d); names.append(f"weighted_t{cap}"); iters.append(cap)
-            algos.append(capi.ALGO_WAMIN); storages.append(st)
-            wsrc[names[-1]] = src
+            for tag in tags:
+                d = capi.Decoder.from_code(code, device)
+                w, src = _weights_for(code, cap, weights, tag)
+                weighted.apply_weights(d, code, w, cap)
+                st, _ = _tune(d, code, mid, cap, capi.ALGO_WAMIN, tune_frames)
+                decs.append(d); names.append(f"weighted_{tag + '_' if tag else ''}t{cap}"); iters.append(cap)
+                algos.append(capi.ALGO_WAMIN); storages.append(st)
+                wsrc[names[-1]] = src
             if controls:  # the plain decoder with the same cap: what the weights add beyond the cap
                 d = capi.Decoder.from_code(code, device)
                 st, _ = _tune(d, code, mid, cap, capi.ALGO_AMIN, tune_frames)
@@ -127,7 +129,7 @@ def compare_code(code: ar4ja.QcCode, points: Sequence[float], frames: int, caps:
                 dd = pt["decoders"][name]
                 dd["fer_matches_plain"] = intervals_overlap(tuple(dd["fer_ci95"]), tuple(base["fer_ci95"]))
                 dd["time_ratio_vs_plain"] = dd["gpu_us_per_frame"] / base["gpu_us_per_frame"]
-                ctl = pt["decoders"].get(name.replace("weighted_", "plain_"))
+                ctl = pt["decoders"].get("plain_" + name.rsplit("_", 1)[-1])
                 if name.startswith("weighted_") and ctl is not None:
                     dd["fer_vs_plain_same_cap"] = dd["fer"] / ctl["fer"] if ctl["fer"] > 0 else None
             out["points"][str(eb)] = pt
@@ -156,6 +158,8 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--weights", default="", help="weights file to use instead of the committed ones")
     ap.add_argument("--no-controls", action="store_true", help="skip the plain decoders capped at each T")
+    ap.add_argument("--tags", nargs="+", default=[""],
+                    help="weight files to compare, by tag (\"\" = the per-edge BCE weights; e.g. check_stop)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     results = []
@@ -164,7 +168,7 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
         code = ar4ja.make_code(int(K), rate)
         results.append(compare_code(code, a.ebn0, a.frames, a.caps, a.time_frames, a.device,
                                     log=lambda s: print(s, flush=True), min_errors=a.min_errors,
-                                    weights=a.weights or None, controls=not a.no_controls))
+                                    weights=a.weights or None, controls=not a.no_controls, tags=a.tags))
     doc = {"seed": SEED, "plain_max_iter": PLAIN_ITERS, "caps": a.caps, "max_frames_per_point": a.frames,
            "min_errors": a.min_errors, "results": results}
     if a.out:

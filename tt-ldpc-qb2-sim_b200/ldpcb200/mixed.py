@@ -4,12 +4,14 @@ Frames are drawn uniformly over the codes (a seeded multinomial split of the tot
 draws its own Eb/N0 uniformly in [threshold + 0.5, threshold + 2.0] dB of its code, where the
 threshold is the PEXIT threshold of the code's protograph (ldpcb200.threshold; the reference does not
 define one).  Each code runs its own persistent kernel - the layered QC kernel for K <= 4096, the
-global-message variant for K = 16384 - and the nine kernels are nodes of one CUDA graph, running side
-by side.  Per code, the autotuner picks the message storage (fp32 / fp16 / bf16) and the launch
-shape (frames per CTA, register cap, paired frames) by timing every built variant, and the graph
-gives each kernel its full persistent grid: the hardware block scheduler starts a code's CTAs as the
-CTAs launched before it retire, so the codes follow one another with their tails overlapped (an
-alternative splits the CTA slots in proportion to each code's expected time).
+global-message variant for K = 16384 - and the nine kernels are nodes of one CUDA graph.  Per code,
+the autotuner picks the message storage (fp32 / fp16 / bf16) and the launch shape (frames per CTA,
+register cap, paired frames) by timing every built variant, and the graph gives each kernel its full
+persistent grid.  ``order`` sets the dependencies between the kernel nodes: "in-turn" (the default:
+each code's kernel has the GPU and its L2 to itself, and the graph takes the sum of the codes' times
+alone), "side-by-side" (no dependencies: the block scheduler interleaves the codes' CTAs) or
+"global-in-turn" (only the global-message kernels chained).  An alternative splits the CTA slots in
+proportion to each code's expected time (``split_sms``).
 """
 from __future__ import annotations
 
@@ -39,7 +41,8 @@ class CodeResult:
 
 class MixedWorkload:
     def __init__(self, codes: Sequence[Tuple[int, str]] = ar4ja.ALL_CODES, device: int = 0, autotune: bool = True,
-                 storages: Sequence[str] = ("fp32", "fp16", "bf16"), tune_symbols: int = 1 << 29, max_iter: int = 200):
+                 storages: Sequence[str] = ("fp32", "fp16", "bf16"), tune_symbols: int = 1 << 29, max_iter: int = 200,
+                 order: str = "in-turn"):
         self.codes = [ar4ja.make_code(K, r) for K, r in codes]
         self.decs = [capi.Decoder.from_code(c, device) for c in self.codes]
         self.ranges = [(threshold.threshold_db(c.rate) + SNR_LOW, threshold.threshold_db(c.rate) + SNR_HIGH)
@@ -71,6 +74,8 @@ class MixedWorkload:
             self.shape.append(tuple(sh))
             self.rate_fps.append(fps)
         self.batch = capi.Batch(self.decs)
+        self.order = order
+        self.batch.set_order(order)
 
     def close(self):
         self.batch.close()
@@ -98,6 +103,20 @@ class MixedWorkload:
             out.append(CodeResult(c.name, r.frames, r.frame_errors, r.bit_errors, r.iter_sum, c.n_tx, rg, st, sh,
                                   d.snr_bins()))
         return out, ms
+
+    def run_alone(self, total_frames: int, seed: int = 1, first_frame: int = 0,
+                  counts: Optional[np.ndarray] = None) -> List[float]:
+        """The frames one ``run`` would decode, each code's share in its own launch with the whole
+        GPU to itself (same frames, per-frame Eb/N0, storage and shape).  Returns each code's kernel
+        ms: their sum against ``run``'s graph time measures what running the codes side by side in
+        one graph gains or loses against running them one after another."""
+        counts = self.split(total_frames, seed) if counts is None else np.asarray(counts)
+        out = []
+        for i, (d, n, st, (lo, hi)) in enumerate(zip(self.decs, counts, self.storage, self.ranges)):
+            p = d.params(seed=seed, stream=i, first_frame=first_frame, n_frames=int(n), max_iter=self.max_iter,
+                         storage=st, ebn0_lo=lo, ebn0_hi=hi)
+            out.append(d.run_chunk(p).kernel_ms if n else 0.0)
+        return out
 
 
 def summarize(results: List[CodeResult], ms: float) -> dict:

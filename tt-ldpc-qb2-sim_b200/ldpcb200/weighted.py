@@ -13,8 +13,12 @@ plain fp32 decoder's values bit for bit.
 Training (``train``) draws its frames from the simulator's own channel (Philox + Box-Muller AWGN,
 all-zero codeword, per-frame Eb/N0 uniform in a range), through ``ldpc_channel_llr_device``, and
 minimises the binary cross-entropy of the posteriors against the all-zero codeword,
-mean(softplus(-L)), averaged over all T iterations' posteriors.  Trained weights run in the
-simulation kernels as LDPC_ALGO_WAMIN (``Decoder.set_weights``), with the syndrome stop.  The
+mean(softplus(-L)), averaged over all T iterations' posteriors (or ``stop_loss``, which rewards
+frames whose hard decisions are all correct early).  Trained weights run in the simulation kernels
+as LDPC_ALGO_WAMIN (``Decoder.set_weights``), with the syndrome tested from the first iteration on.
+Weights come per protograph edge (``granularity="edge"``) or per protograph check row ("check"): the
+second kind is applied once per row, so its decoder costs little more per iteration than the plain
+one.  The
 reference has no weighted or trainable decoder; nothing here has a counterpart there.
 """
 from __future__ import annotations
@@ -36,20 +40,34 @@ TRAIN_STREAM = 0x7EA1
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 
 
-def edge_class_table(code: ar4ja.QcCode) -> np.ndarray:
-    """[12][18] int32: class of edge e of layer l (0 beyond the layer's degree)."""
+GRANULARITIES = ("edge", "check")
+
+
+def n_classes(code: ar4ja.QcCode, granularity: str = "edge") -> int:
+    """Parameters per iteration: one per protograph edge ("edge"), or one per protograph check row
+    ("check": the three block rows of every AR4JA base matrix, each lifted to four layers)."""
+    if granularity not in GRANULARITIES:
+        raise ValueError(f"granularity must be one of {GRANULARITIES}")
+    return code.n_classes if granularity == "edge" else len(code.layers) // 4
+
+
+def edge_class_table(code: ar4ja.QcCode, granularity: str = "edge") -> np.ndarray:
+    """[12][18] int32: class of edge e of layer l (0 beyond the layer's degree).  "check": every edge
+    of layer l in class l // 4, its protograph check row; the simulation kernels then apply the
+    weights once per row (the per-row weighted kernels) instead of once per edge."""
+    n_classes(code, granularity)
     t = np.zeros((12, 18), np.int32)
     for l, cls in enumerate(code.edge_class):
-        t[l, :len(cls)] = cls
+        t[l, :len(cls)] = cls if granularity == "edge" else l // 4
     return t
 
 
 def make_config(code: ar4ja.QcCode, n_iter: int, ckpt_every: int = 5, post_all: bool = True,
-                fp64: bool = False) -> capi.WdecConfig:
+                fp64: bool = False, granularity: str = "edge") -> capi.WdecConfig:
     c = capi.WdecConfig()
-    c.n_iter, c.n_classes, c.ckpt_every = int(n_iter), int(code.n_classes), int(min(ckpt_every, n_iter))
+    c.n_iter, c.n_classes, c.ckpt_every = int(n_iter), int(n_classes(code, granularity)), int(min(ckpt_every, n_iter))
     c.post_all, c.fp64 = int(bool(post_all)), int(bool(fp64))
-    tab = edge_class_table(code)
+    tab = edge_class_table(code, granularity)
     for l in range(12):
         for e in range(18):
             c.edge_class[l][e] = int(tab[l, e])
@@ -111,16 +129,18 @@ def extend(w: torch.Tensor, n_iter: int) -> torch.Tensor:
 
 class WeightedDecoder(torch.nn.Module):
     """Trainable weighted decoder of one AR4JA code (makeH row order): parameters alpha and beta of
-    shape [T][C], initialised to 1 and 0 (the plain decoder)."""
+    shape [T][C], initialised to 1 and 0 (the plain decoder); C classes per ``granularity``."""
 
     def __init__(self, code: ar4ja.QcCode, n_iter: int = 20, ckpt_every: int = 5, device: int = 0,
-                 dtype: torch.dtype = torch.float32, post_all: bool = True):
+                 dtype: torch.dtype = torch.float32, post_all: bool = True, granularity: str = "edge"):
         super().__init__()
         self.code, self.n_iter, self.device = code, int(n_iter), torch.device("cuda", device)
+        self.granularity = granularity
+        nc = n_classes(code, granularity)
         self.dec = capi.Decoder.from_code(code, device)
-        self.cfg = make_config(code, n_iter, ckpt_every, post_all, dtype == torch.float64)
-        self.alpha = torch.nn.Parameter(torch.ones(n_iter, code.n_classes, dtype=dtype, device=self.device))
-        self.beta = torch.nn.Parameter(torch.zeros(n_iter, code.n_classes, dtype=dtype, device=self.device))
+        self.cfg = make_config(code, n_iter, ckpt_every, post_all, dtype == torch.float64, granularity)
+        self.alpha = torch.nn.Parameter(torch.ones(n_iter, nc, dtype=dtype, device=self.device))
+        self.beta = torch.nn.Parameter(torch.zeros(n_iter, nc, dtype=dtype, device=self.device))
 
     def forward(self, llr: torch.Tensor) -> torch.Tensor:
         return WeightedFn.apply(llr, self.alpha, self.beta, self.dec, self.cfg)
@@ -144,7 +164,7 @@ class WeightedDecoder(torch.nn.Module):
 
     def state(self) -> dict:
         return {"code": self.code.name, "K": self.code.K, "rate": self.code.rate, "n_iter": self.n_iter,
-                "n_classes": self.code.n_classes,
+                "granularity": self.granularity, "n_classes": n_classes(self.code, self.granularity),
                 "alpha": self.alpha.detach().double().cpu().numpy().round(7).tolist(),
                 "beta": self.beta.detach().double().cpu().numpy().round(7).tolist()}
 
@@ -167,6 +187,20 @@ def bce_allzero(post: torch.Tensor, iters: Optional[Tuple[int, int]] = None) -> 
     return torch.nn.functional.softplus(-post).mean()
 
 
+def stop_loss(post: torch.Tensor) -> torch.Tensor:
+    """A loss for stopping early: with S[t, b] = sum over the bits of softplus(-post), exp(-S) is the
+    probability, under independent bit posteriors, that frame b's hard decisions after iteration t
+    are all correct (the all-zero codeword, where the syndrome test stops it).  The mean over
+    iterations of 1 - exp(-S) estimates the expected fraction of the T iterations a frame still runs,
+    so its gradient goes to the frames about to converge; the mean bit BCE is added so frames far from
+    convergence still pull the posteriors the right way."""
+    S = torch.nn.functional.softplus(-post).sum(-1)  # [T][B]
+    return (1.0 - torch.exp(-S)).mean() + torch.nn.functional.softplus(-post).mean()
+
+
+LOSSES = {"bce": lambda post, iters: bce_allzero(post, iters), "stop": lambda post, iters: stop_loss(post)}
+
+
 @dataclass
 class TrainLog:
     step: int
@@ -177,24 +211,26 @@ class TrainLog:
 def train(code: ar4ja.QcCode, steps: int = 5000, batch: int = 4096, ebn0: Tuple[float, float] = (1.0, 2.5),
           lr: float = 1e-3, n_iter: int = 20, ckpt_every: int = 5, seed: int = 1, device: int = 0,
           log_every: int = 100, callback: Optional[Callable[[TrainLog], None]] = None,
-          loss_iters: Optional[Tuple[int, int]] = None) -> Tuple[WeightedDecoder, list]:
-    """Adam on mean BCE over all iterations' posteriors (or those of loss_iters, 1-based inclusive);
-    step i decodes frames i * batch .. of the training channel stream, so every step sees fresh
-    frames."""
+          loss_iters: Optional[Tuple[int, int]] = None, granularity: str = "edge",
+          loss: str = "bce") -> Tuple[WeightedDecoder, list]:
+    """Adam on mean BCE over all iterations' posteriors (or those of loss_iters, 1-based inclusive),
+    or on ``stop_loss`` (loss="stop"); step i decodes frames i * batch .. of the training channel
+    stream, so every step sees fresh frames."""
     torch.cuda.set_device(device)
-    model = WeightedDecoder(code, n_iter, ckpt_every, device)
+    lossf = LOSSES[loss]
+    model = WeightedDecoder(code, n_iter, ckpt_every, device, granularity=granularity)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     llr = torch.empty((batch, model.dec.n_tx), dtype=torch.float32, device=model.device)
     log = []
     t0 = time.time()
     for step in range(steps):
         model.channel(batch, ebn0, seed, first_frame=step * batch, out=llr)
-        loss = bce_allzero(model(llr), loss_iters)
+        lv = lossf(model(llr), loss_iters)
         opt.zero_grad(set_to_none=True)
-        loss.backward()
+        lv.backward()
         opt.step()
         if log_every and (step % log_every == 0 or step == steps - 1):
-            entry = TrainLog(step, float(loss.item()), time.time() - t0)
+            entry = TrainLog(step, float(lv.item()), time.time() - t0)
             log.append(entry)
             if callback:
                 callback(entry)
@@ -202,8 +238,11 @@ def train(code: ar4ja.QcCode, steps: int = 5000, batch: int = 4096, ebn0: Tuple[
     return model, log
 
 
-def weights_path(code: ar4ja.QcCode, n_iter: int) -> str:
-    return os.path.join(WEIGHTS_DIR, f"ar4ja_r{code.rate.replace('/', '')}_k{code.K}_t{n_iter}.json")
+def weights_path(code: ar4ja.QcCode, n_iter: int, tag: str = "") -> str:
+    """ar4ja_r<rate>_k<K>_t<T>[_<tag>].json under the package's weights folder (tag names a
+    granularity or loss other than per-edge weights trained on BCE)."""
+    suffix = f"_{tag}" if tag else ""
+    return os.path.join(WEIGHTS_DIR, f"ar4ja_r{code.rate.replace('/', '')}_k{code.K}_t{n_iter}{suffix}.json")
 
 
 def save_weights(model: WeightedDecoder, path: str, extra: Optional[dict] = None):
@@ -227,7 +266,7 @@ def apply_weights(dec: capi.Decoder, code: ar4ja.QcCode, st: dict, n_iter: Optio
     if n_iter:
         a = extend(torch.from_numpy(a), n_iter).numpy()
         b = extend(torch.from_numpy(b), n_iter).numpy()
-    dec.set_weights(a, b, edge_class_table(code))
+    dec.set_weights(a, b, edge_class_table(code, st.get("granularity", "edge")))
 
 
 def _main(argv: Optional[Sequence[str]] = None):
@@ -245,15 +284,20 @@ def _main(argv: Optional[Sequence[str]] = None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--loss-iters", type=int, nargs=2, default=None,
                     help="train on the posteriors of these iterations only (1-based, inclusive)")
+    ap.add_argument("--granularity", choices=GRANULARITIES, default="edge",
+                    help="one (alpha, beta) per protograph edge, or per protograph check row")
+    ap.add_argument("--loss", choices=tuple(LOSSES), default="bce")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     code = ar4ja.make_code(a.K, a.rate)
     li = tuple(a.loss_iters) if a.loss_iters else None
     model, log = train(code, a.steps, a.batch, tuple(a.ebn0), a.lr, a.iters, a.ckpt_every, a.seed, a.device,
-                       callback=lambda e: print(json.dumps(e.__dict__), flush=True), loss_iters=li)
-    out = a.out or weights_path(code, a.iters)
+                       callback=lambda e: print(json.dumps(e.__dict__), flush=True), loss_iters=li,
+                       granularity=a.granularity, loss=a.loss)
+    tag = "_".join(x for x in (a.granularity if a.granularity != "edge" else "", a.loss if a.loss != "bce" else "") if x)
+    out = a.out or weights_path(code, a.iters, tag)
     save_weights(model, out, {"train": {"steps": a.steps, "batch": a.batch, "ebn0_db": list(a.ebn0), "lr": a.lr,
-                                        "ckpt_every": a.ckpt_every, "seed": a.seed,
+                                        "ckpt_every": a.ckpt_every, "seed": a.seed, "loss_fn": a.loss,
                                         "loss_iters": list(li) if li else "all",
                                         "loss": [[e.step, round(e.loss, 6)] for e in log],
                                         "seconds": round(log[-1].seconds, 2) if log else 0.0}})
