@@ -216,6 +216,22 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU baseline
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+REF_BUILD = ("g++ -O3 -ffp-contract=off (oracle/Makefile; the reference's own build line has no -march, so "
+             "no -march=native here either)")
+
+
 def cpu_baseline(seconds: float, threads: int = 0, code=None):
     """The reference's own decoder (oracle/_ref/ref_mc) on every host thread, else the oracle port."""
     from oracle import oracle as O
@@ -239,6 +255,7 @@ def cpu_baseline(seconds: float, threads: int = 0, code=None):
     fps = frames / el if el > 0 else 0.0
     return {
         "value": round(fps * code.n_tx / 1e9, 6), "unit": UNIT, "cores": threads, "kind": kind,
+        "cpu_model": cpu_model(), "build": REF_BUILD if kind == "reference" else "oracle port",
         "frames_per_s": round(fps, 1),
         "sample": (f"{frames} frames over {el:.1f} s: Eb/N0 {POINTS[0]} and {POINTS[1]} dB, "
                    f"{per_point:.0f} s each, max {MAX_ITER} iterations, bf16 reference numerics, "
@@ -308,6 +325,7 @@ def run_reference(args):
                    "engine": "run_ldpc_worker (engines/scalar_5w/ldpc_decoder_core.h) on host threads",
                    "frames_per_s": round(frames / el, 1) if el > 0 else 0.0, "fer": fe / max(frames, 1)},
         "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": kind,
+                         "cpu_model": cpu_model(), "build": REF_BUILD if kind == "reference" else "oracle port",
                          "sample": f"{frames} frames over {el:.1f} s in {args.steps} steps of "
                                    f"{args.ref_step_seconds:.1f} s per Eb/N0 point"},
         "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1034,6 +1052,7 @@ def run_reference_circulant(args):
                              "on host threads",
                    "frames_per_s": round(frames / el, 1) if el > 0 else 0.0, "fer": fe / max(frames, 1)},
         "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": f"{frames} frames over {el:.1f} s in {args.steps} steps of about "
                                    f"{args.ref_step_seconds:.1f} s per Eb/N0 point"},
         "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -126,6 +126,15 @@ int ldpc_kernel_kind(const ldpc_handle* h);
  * error for a bad matrix. */
 int ldpc_row_schedule(const ldpc_matrix* h, int32_t* order, int32_t* starts);
 
+/* The schedule the step kernel (the general kernel for rows of degree at most 10, the one the shipped
+ * matrix file runs on) uses instead (host only, needs no GPU).  The same rule keeps the file order of
+ * every pair of rows sharing a variable, but each step takes rows of one degree class: low (degree
+ * at most half the kernel's degree bound: 3 for files of degree up to 6) or high, so that a low step
+ * runs the kernel's short row body.  Steps are filled by list scheduling, the rows with the longest
+ * chain of dependants first.  Writes order[M], starts[M + 1] (as ldpc_row_schedule) and low[M]
+ * (1 for a low step, one entry per step); returns the number of steps, or a negative error. */
+int ldpc_step_schedule(const ldpc_matrix* h, int32_t* order, int32_t* starts, int32_t* low);
+
 /* Simulates p->n_frames frames (channel generation, decoding, tallies) on the device; replaces one
  * batch of ldpc_sim_scalar.cpp:421-589 (EnqueueMeshWorkload + ReadShard + host sums).  Blocks until
  * the tallies are on the host. */
@@ -172,7 +181,10 @@ int ldpc_snr_bins(ldpc_handle* h, uint64_t* out);
  * frames per CTA, the resident CTAs per SM its register allocation must allow (a register cap;
  * 0 = the compiler's choice), and the layout (global_messages): 0 = check messages in registers,
  * 1 = in global memory (codes too large for the register file), 2 = in registers, with each
- * thread's column offsets precomputed in shared memory.  All zero restores the default.
+ * thread's column offsets precomputed in shared memory, 5 = as 1 with the code's layer descriptors
+ * compiled into the kernel (built for the K = 16384 AR4JA codes in makeH order, offered only when
+ * the matrix's descriptors are exactly those; layouts 3 and 4 are the general kernels').  All zero
+ * restores the default.
  * LDPC_ENOTSUP if the shape is not built for this code.  Used by the autotuner
  * (ldpcb200.capi.Decoder.autotune).  Options with no QC variant built (e.g. clips on a K = 16384
  * code) run on the general kernel. */

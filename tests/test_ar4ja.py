@@ -171,3 +171,15 @@ def test_circulant_tile_slices_decode_exactly_h():
                 for c in range(16):
                     m = 64 * (t - 32) + 16 * fi + c
                     assert [nodes(face[t][d])[c] for d in range(3)] == rows[m], (t, m)
+
+
+def test_fixed_table_header_is_current():
+    """csrc/ar4ja_fixed_tables.h (the layer descriptors compiled into the K = 16384 layout-5 kernels)
+    is what ldpcb200.fixed_tables writes from the makeH construction."""
+    from ldpcb200 import fixed_tables
+    assert fixed_tables.main(["--check"]) == 0
+    for i, (K, rate) in enumerate(fixed_tables.CODES):
+        Z, D, blk, sh = fixed_tables.descriptors(ar4ja.make_code(K, rate))
+        code = ar4ja.make_code(K, rate)
+        for l, layer in enumerate(code.layers):  # (block, shift) pairs in ascending block order
+            assert [(b * Z, s) for b, s in layer] == list(zip(blk[l], sh[l]))[:len(layer)]

@@ -95,3 +95,67 @@ def test_schedule_order_decodes_as_the_file_order(golden, mode):
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
     assert (a[2] > 0).any() and (a[2] == 0).any()  # some frames stop, some do not
+
+
+# The step kernel's schedule (ldpc_step_schedule): the same ordering rule, steps of one degree class.
+
+def _check_classes(rows, order, starts, low, dl):
+    deg = (rows >= 0).sum(1)
+    for k in range(len(starts) - 1):
+        d = deg[np.array(order[starts[k]:starts[k + 1]])]
+        assert (d <= dl).all() if low[k] else (d > dl).all(), k
+
+
+def test_step_schedule_of_the_shipped_file(golden):
+    """512 rows of degree 3 and 1024 of degree 6: 54 steps (18 of degree 3, 36 of degree 6, against
+    the 16 and 32 that full steps would need) in place of the row schedule's 51 mixed steps."""
+    rows, N, _ = golden_matrix(golden, "shipped")
+    order, starts, low = capi.step_schedule(rows, N)
+    _check_schedule(rows, order, starts)
+    _check_classes(rows, order, starts, low, 3)
+    assert len(starts) - 1 == 54 and int(low.sum()) == 18
+    o2, s2, l2 = chinn.step_schedule(_matrix(rows, N), 3)
+    assert order.tolist() == o2 and starts.tolist() == s2 and low.tolist() == l2
+
+
+def test_step_schedule_equals_restatement():
+    rng = np.random.default_rng(5)
+    cases = []
+    for K, rate in ((1024, "1/2"), (1024, "4/5"), (4096, "2/3")):
+        c = ar4ja.make_code(K, rate)
+        if c.row_matrix().shape[1] <= 10:
+            cases.append((c.row_matrix(), c.N))
+    for _ in range(6):  # random ragged matrices, degrees 0-10
+        N, M, d = int(rng.integers(20, 300)), int(rng.integers(5, 400)), int(rng.integers(1, 11))
+        rows = np.full((M, d), -1, np.int32)
+        for m in range(M):
+            k = int(rng.integers(0, d + 1))
+            rows[m, :k] = rng.choice(N, size=k, replace=False)
+        cases.append((rows, N))
+    for rows, N in cases:
+        maxdeg = int((rows >= 0).sum(1).max())
+        dl = (6 if maxdeg <= 6 else 8 if maxdeg <= 8 else 10) // 2
+        order, starts, low = capi.step_schedule(rows, N)
+        o2, s2, l2 = chinn.step_schedule(_matrix(rows, N), dl)
+        assert order.tolist() == o2 and starts.tolist() == s2 and low.tolist() == l2
+        _check_schedule(rows, order, starts)
+        _check_classes(rows, order, starts, low, dl)
+
+
+def test_step_schedule_rejects_rows_above_degree_10():
+    rows = np.arange(11, dtype=np.int32)[None, :]
+    with pytest.raises(capi.LdpcError):
+        capi.step_schedule(rows, 20)
+
+
+@pytest.mark.parametrize("mode", [O.STORE_BF16, O.STORE_FP32])
+def test_step_schedule_order_decodes_as_the_file_order(golden, mode):
+    rows, N, P = golden_matrix(golden, "shipped")
+    order, _, _ = capi.step_schedule(rows, N)
+    rng = np.random.default_rng(12)
+    mu, sigma = capi.channel_mu_sigma(N, rows.shape[0], P, 1.0)
+    llr = (mu + sigma * rng.standard_normal((6, N - P))).astype(np.float32)
+    a = O.decode(O.Code(rows, N, P), llr, mode=mode, max_iter=30)
+    b = O.decode(O.Code(rows[np.array(order)], N, P), llr, mode=mode, max_iter=30)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

@@ -367,7 +367,7 @@ int build_general(const int32_t* rows, int N, int M, int P, int dmax, GeneralCod
     if (cudaMemcpy(g->d_cols, cols.data(), cols.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(g->d_runs, runs.data(), runs.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
         return gfail(err, LDPC_EIO, "copy of the matrix to the device failed");
-    return build_general_steps(rows, dmax, order, runs, g, err);
+    return build_general_steps(rows, dmax, g, err);
 }
 
 void free_general(GeneralCode* g) {
@@ -378,6 +378,8 @@ void free_general(GeneralCode* g) {
     cudaFree(g->d_scols[1]);
     cudaFree(g->d_slot[0]);
     cudaFree(g->d_slot[1]);
+    cudaFree(g->d_slow);
+    g->d_slow = nullptr;
     g->d_cols = g->d_runs = nullptr;
     g->d_scols[0] = g->d_scols[1] = nullptr;
     g->d_slot[0] = g->d_slot[1] = nullptr;

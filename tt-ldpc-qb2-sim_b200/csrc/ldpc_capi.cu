@@ -72,6 +72,7 @@ struct ldpc_handle {
     int Z = 0, D = 0;
     int32_t blk_off[QC_LAYERS][QC_DMAX] = {};
     int32_t shift[QC_LAYERS][QC_DMAX] = {};
+    int fix = -1;  // index of kQcFixedHost holding exactly these descriptors (layout 5 kernels), or -1
     // per storage mode: rows per thread, frames per CTA, min CTAs/SM, messages in global memory;
     // all zero = the default shape
     int shape[3][4] = {};
@@ -159,6 +160,16 @@ static int detect_qc(ldpc_handle* h) {
     }
     h->Z = Z;
     h->D = D;
+    // a code whose descriptors some kernels have compiled in (layout 5)
+    h->fix = -1;
+    for (int i = 0; i < QC_FIXED_COUNT && h->fix < 0; ++i) {
+        const QcFixedTable& t = kQcFixedHost[i];
+        bool same = t.Z == Z && t.D == D;
+        for (int l = 0; l < QC_LAYERS && same; ++l)
+            for (int e = 0; e < (l < 4 ? QC_DEG_LOW : D) && same; ++e)
+                same = t.blk_off[l][e] == h->blk_off[l][e] && t.shift[l][e] == h->shift[l][e];
+        if (same) h->fix = i;
+    }
     return 1;
 }
 
@@ -296,6 +307,25 @@ extern "C" int ldpc_row_schedule(const ldpc_matrix* m, int32_t* order, int32_t* 
     return (int)st.size() - 1;
 }
 
+extern "C" int ldpc_step_schedule(const ldpc_matrix* m, int32_t* order, int32_t* starts, int32_t* low) {
+    if (!low) return fail(LDPC_EINVAL, "matrix or output is NULL");
+    int rc = ldpc_row_schedule(m, order, starts);  // argument checks (and a scratch use of the outputs)
+    if (rc < 0) return rc;
+    int maxdeg = 0;
+    for (int i = 0; i < m->n_checks; ++i)
+        for (int e = 0; e < m->max_check_deg && m->rows[(size_t)i * m->max_check_deg + e] >= 0; ++e)
+            maxdeg = std::max(maxdeg, e + 1);
+    const int dt = step_dt(maxdeg);
+    if (!dt) return fail(LDPC_ENOTSUP, "rows of degree %d: the step kernel takes degrees up to 10", maxdeg);
+    std::vector<int32_t> o, st;
+    std::vector<uint8_t> lo;
+    step_schedule(m->rows, m->n_vars, m->n_checks, m->max_check_deg, dt / 2, o, st, lo);
+    std::copy(o.begin(), o.end(), order);
+    std::copy(st.begin(), st.end(), starts);
+    std::copy(lo.begin(), lo.end(), low);
+    return (int)st.size() - 1;
+}
+
 extern "C" int ldpc_kernel_kind(const ldpc_handle* h) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
     return h->kind;
@@ -309,6 +339,7 @@ extern "C" int64_t ldpc_launch_param_bytes(const ldpc_handle* h) {
 }
 
 static const void* find_shape(const ldpc_handle* h, int storage, int algo, int clip, int ext, int R, int F, int B, int G) {
+    if (G == 5 && h->fix < 0) return nullptr;  // compiled-in descriptors of another code
     return find_qc(QcKey{h->Z, h->D, R, F, storage, algo, clip, ext, B, G});
 }
 
@@ -323,7 +354,8 @@ static bool default_shape(const ldpc_handle* h, int storage, int algo, int clip,
     for (const QcTable* t = qc_tables(); t; t = t->next)
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
-            if (k.Z == h->Z && k.D == h->D && k.mode == storage && k.algo == algo && k.clip == clip && k.ext == ext) {
+            if (k.Z == h->Z && k.D == h->D && k.mode == storage && k.algo == algo && k.clip == clip && k.ext == ext &&
+                (k.G != 5 || h->fix >= 0)) {
                 s[0] = k.R; s[1] = k.F; s[2] = k.B; s[3] = k.G;
                 return true;
             }
@@ -423,7 +455,7 @@ static bool general_shape_ok(const ldpc_handle* h, int R, int F, int B, int G) {
 
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 4)
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 5)
         return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
@@ -438,7 +470,7 @@ extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, 
         }
         return 0;
     }
-    if (G > 2) return fail(LDPC_ENOTSUP, "layouts 3 and 4 are the general kernels'");
+    if (G == 3 || G == 4) return fail(LDPC_ENOTSUP, "layouts 3 and 4 are the general kernels'");
     bool any = reset;
     auto built = [&](int s) {
         return find_shape(h, s, LDPC_ALGO_AMIN, 0, 0, R, F, B, G) || find_shape(h, s, LDPC_ALGO_WAMIN, 0, 0, R, F, B, G) ||
@@ -483,6 +515,7 @@ extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
             if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != algo || k.clip || k.ext) continue;
+            if (k.G == 5 && h->fix < 0) continue;
             if (n < max_shapes) {
                 shapes[4 * n] = k.R;
                 shapes[4 * n + 1] = k.F;
@@ -653,7 +686,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     out->block = T;
     out->smem = smem;
     if (grid == 0) return 0;
-    if (G == 1) {
+    if (G == 1 || G == 5) {
         int rc;
         const size_t rsz = p->storage == LDPC_STORE_FP32 ? 4 : 2;
         if ((rc = ensure_cap(&h->d_rmsg, &h->rmsg_cap, grid * F * (size_t)qp.slot_elems * rsz))) return rc;

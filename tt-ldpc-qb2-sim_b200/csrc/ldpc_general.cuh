@@ -38,6 +38,8 @@ struct GeneralCode {
     int sdt = 0;                          // its degree bound (0: the matrix needs the warp kernel)
     int32_t* d_scols[2] = {nullptr, nullptr};  // byte offsets for 2- and 4-byte posteriors, step_table layout
     int32_t* d_slot[2] = {nullptr, nullptr};   // [N] the shared-memory slot of each variable, per element size
+    int s_steps = 0;                      // steps of the step kernel's own schedule (step_schedule)
+    int32_t* d_slow = nullptr;            // [s_steps] 1: every row of the step has degree <= sdt / 2
     int step_ctas = 0;                    // step kernel CTAs per SM (0: as many as fit)
 };
 
@@ -63,6 +65,7 @@ struct GenParams {
     unsigned long long* snr_bins;
     const int32_t* scols;                 // step kernel: its column table (byte offsets)
     const int32_t* slot;                  // step kernel: [N] shared-memory slot of each variable
+    const int32_t* slow;                  // step kernel: [n_steps] 1 for a step of low-degree rows
     int32_t n_steps;
 };
 
@@ -74,9 +77,15 @@ void free_general(GeneralCode* g);
 int decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr, int64_t n,
                       float* d_post, int32_t* d_iters, int32_t* d_synd, int32_t* d_be, ldpc_tally* out,
                       cudaStream_t stream, std::string& err);
-// Builds the step kernel's tables for the schedule (order, starts) of build_general.
-int build_general_steps(const int32_t* rows, int dmax, const std::vector<int32_t>& order,
-                        const std::vector<int32_t>& starts, GeneralCode* g, std::string& err);
+// The step kernel's degree bound for rows of at most maxdeg edges (6, 8 or 10), or 0 when the
+// matrix needs the warp kernel.
+int step_dt(int maxdeg);
+// The step kernel's schedule (general_step.cu): steps of up to 32 rows of one degree class (low:
+// degree <= dl), each row after the earlier rows it shares a variable with.  low[s] = 1 for a low step.
+void step_schedule(const int32_t* rows, int N, int M, int dmax, int dl, std::vector<int32_t>& order,
+                   std::vector<int32_t>& starts, std::vector<uint8_t>& low);
+// Builds the step kernel's schedule and tables for the matrix of build_general.
+int build_general_steps(const int32_t* rows, int dmax, GeneralCode* g, std::string& err);
 // The step kernel; LDPC_ENOTSUP when it does not run these numerics or this matrix (the caller then
 // takes the warp kernel).
 int launch_general_step(GeneralCode* g, const ldpc_run_params* p, bool ext, uint32_t n, uint64_t first,

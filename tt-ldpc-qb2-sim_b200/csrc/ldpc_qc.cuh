@@ -22,6 +22,7 @@
 // frame counter: early-retire with slot refill, so fast and slow frames never wait for each other.
 #pragma once
 #include <cstdint>
+#include "ar4ja_fixed_tables.h"
 #include "ldpc_device.cuh"
 
 namespace ldpcb200 {
@@ -555,6 +556,20 @@ __device__ __forceinline__ void ot_load(const uint32_t* tab, int t, int* idx) {
     if constexpr (rem & 1) idx[d - 1] = (int)tab[T * (c4 + (rem >= 2 ? 2 : 0)) + t];
 }
 
+// Edge e of layer l: column block offset (block * Z) and circulant shift, from the launch parameters
+// or, for FIX >= 0, compiled in (the descriptors of code kQcFixedDev[FIX]; in the unrolled layer loop
+// they become immediate operands).
+template <int FIX>
+__device__ __forceinline__ int qc_blk(const QcParams& p, int l, int e) {
+    if constexpr (FIX >= 0) return kQcFixedDev[FIX].blk_off[l][e];
+    else return p.blk_off[l][e];
+}
+template <int FIX>
+__device__ __forceinline__ int qc_shift(const QcParams& p, int l, int e) {
+    if constexpr (FIX >= 0) return kQcFixedDev[FIX].shift[l][e];
+    else return p.shift[l][e];
+}
+
 // B: resident CTAs per SM the register allocation must allow (0 = the compiler's choice); a larger B
 // caps registers per thread at 65536 / (B * Z/R) and trades registers for resident warps.
 // PAIR: the paired mode above (F = 2, R = 1, 16-bit storage, Approximate-Min*, no clips).
@@ -562,8 +577,10 @@ __device__ __forceinline__ void ot_load(const uint32_t* tab, int t, int* idx) {
 // registers, for codes whose rows per thread times degrees exceed the register file (K = 16384).
 // OT: the column offset table above, built once per CTA in shared memory after the hard-decision
 // words (T * (12 + 8 D) words); one row per thread.
+// FIX: >= 0 for the descriptors of a known code compiled in (global-message kernels of the K = 16384
+// codes; the host offers them only for a matrix whose descriptors are those).
 template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false,
-          bool RG = false, bool OT = false>
+          bool RG = false, bool OT = false, int FIX = -1>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
@@ -573,6 +590,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                   "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
     using RE = typename RTraits<MODE>::T;
     static_assert(!OT || (!PAIR && !RG && R == 1), "the offset table is built for one row per thread");
+    static_assert(FIX < 0 || (RG && FIX < QC_FIXED_COUNT), "compiled-in descriptors: global-message kernels");
     constexpr bool CIRC = ALGO == ALGO_CIRC;
     static_assert(!CIRC || (D == 6 && !CLIP && !PAIR), "the circulant engine's decoder: degrees 3 and 6, no clips");
     using SV = SlotView<MODE, PAIR>;
@@ -741,7 +759,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         } else
 #pragma unroll
                             for (int e = 0; e < QC_DEG_LOW; ++e)
-                                idx[e] = p.blk_off[ly][e] + ((j + p.shift[ly][e]) & (Z - 1));
+                                idx[e] = qc_blk<FIX>(p, ly, e) + ((j + qc_shift<FIX>(p, ly, e)) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<QC_DEG_LOW, MODE> rm[F];
 #pragma unroll
@@ -766,7 +784,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                             for (int e = 0; e < D; ++e) idx[e] = cur[e];
                         } else
 #pragma unroll
-                            for (int e = 0; e < D; ++e) idx[e] = p.blk_off[ly][e] + ((j + p.shift[ly][e]) & (Z - 1));
+                            for (int e = 0; e < D; ++e)
+                                idx[e] = qc_blk<FIX>(p, ly, e) + ((j + qc_shift<FIX>(p, ly, e)) & (Z - 1));
                         if constexpr (RG) {
                             RowMsgGlobal<D, MODE> rm[F];
 #pragma unroll
@@ -834,7 +853,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                             uint32_t par = 0;
 #pragma unroll
                             for (int e = 0; e < dl; ++e)
-                                par ^= L.sign(p.blk_off[l][e] + ((j + p.shift[l][e]) & (Z - 1)));
+                                par ^= L.sign(qc_blk<FIX>(p, l, e) + ((j + qc_shift<FIX>(p, l, e)) & (Z - 1)));
                             bad |= par;
                         }
                     }

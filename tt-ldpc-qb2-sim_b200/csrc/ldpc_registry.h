@@ -9,7 +9,8 @@ namespace ldpcb200 {
 struct QcKey {
     int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
     int G;                                     // layout: 0 registers, 1 messages in global memory (RG
-                                               // kernel), 2 registers + column offset table (OT)
+                                               // kernel), 2 registers + column offset table (OT),
+                                               // 5 as 1 with a known code's descriptors compiled in
     // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
     // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
@@ -43,6 +44,12 @@ const QcTable* qc_tables();
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 1},                                \
      reinterpret_cast<const void*>(                                            \
          &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true>)}
+
+// Layout 5: the global-message kernel with the layer descriptors of fixed-table code FIX compiled in.
+#define LDPC_QC_ENTRY_GF(Z, D, R, F, MODE, ALGO, CLIP, EXT, B, FIX)           \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 5},                                \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true, false, FIX>)}
 
 #define LDPC_QC_ENTRY_OT(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                 \
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 2},                                \

@@ -25,5 +25,16 @@ static const QcEntry qc_k16[] = {
     LDPC_QC_ENTRY_G(1024, 10, 2, 1, STORE_FP16, ALGO_AMIN, false, false, 2),
     LDPC_QC_ENTRY_G(512, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 2),
     LDPC_QC_ENTRY_G(512, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 2),
+    // layout 5: the same kernels with the code's layer descriptors compiled in (ar4ja_fixed_tables.h:
+    // 0 = rate 1/2, 1 = rate 2/3, 2 = rate 4/5), so a circulant index costs no constant-bank operands
+    LDPC_QC_ENTRY_GF(2048, 6, 4, 1, STORE_BF16, ALGO_AMIN, false, false, 0, 0),
+    LDPC_QC_ENTRY_GF(2048, 6, 4, 1, STORE_FP16, ALGO_AMIN, false, false, 0, 0),
+    LDPC_QC_ENTRY_GF(2048, 6, 4, 1, STORE_BF16, ALGO_AMIN, false, true, 0, 0),
+    LDPC_QC_ENTRY_GF(1024, 10, 2, 1, STORE_BF16, ALGO_AMIN, false, false, 0, 1),
+    LDPC_QC_ENTRY_GF(1024, 10, 2, 1, STORE_BF16, ALGO_AMIN, false, false, 2, 1),
+    LDPC_QC_ENTRY_GF(1024, 10, 2, 1, STORE_FP16, ALGO_AMIN, false, false, 2, 1),
+    LDPC_QC_ENTRY_GF(512, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0, 2),
+    LDPC_QC_ENTRY_GF(512, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 2, 2),
+    LDPC_QC_ENTRY_GF(512, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 2, 2),
 };
 LDPC_QC_REGISTER(qc_k16)

@@ -31,7 +31,8 @@ EXPORTS = ("ldpc_create", "ldpc_destroy", "ldpc_kernel_kind", "ldpc_run_chunk", 
            "ldpc_wdec_workspace_bytes", "ldpc_wdec_forward", "ldpc_wdec_backward",
            "ldpc_launch_count", "ldpc_batch_create", "ldpc_batch_destroy", "ldpc_batch_run",
            "ldpc_batch_graph_builds", "ldpc_batch_set_order",
-           "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_row_schedule", "ldpc_last_error",
+           "ldpc_launch_param_bytes", "ldpc_decode_llr_static", "ldpc_row_schedule", "ldpc_step_schedule",
+           "ldpc_last_error",
            "ldpc_abi_version")
 
 
@@ -113,6 +114,8 @@ def load(path: str = LIB_PATH):
     L.ldpc_batch_graph_builds.argtypes = [C.c_void_p]
     L.ldpc_batch_graph_builds.restype = C.c_int64
     L.ldpc_batch_set_order.argtypes = [C.c_void_p, C.c_int]
+    L.ldpc_step_schedule.argtypes = [C.POINTER(Matrix), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)]
     L.ldpc_set_launch_shape.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.ldpc_list_shapes.argtypes = [C.c_void_p, C.c_int, P(C.c_int32), C.c_int]
     L.ldpc_list_shapes_algo.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int32), C.c_int]
@@ -198,6 +201,20 @@ def row_schedule(rows: np.ndarray, n_vars: int):
     starts = np.zeros(M + 1, np.int32)
     n = _check(lib.ldpc_row_schedule(C.byref(m), _ip(order), _ip(starts)))
     return order, starts[:n + 1].copy()
+
+
+def step_schedule(rows: np.ndarray, n_vars: int):
+    """ldpc_step_schedule (host only, no GPU): the step kernel's schedule of a [M, dmax] row table,
+    steps of one degree class.  Returns (order, starts, low): low[s] = 1 for a step of low-degree rows."""
+    lib = load()
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    M = rows.shape[0]
+    m = Matrix(int(n_vars), M, 0, rows.shape[1], _ip(rows))
+    order = np.zeros(M, np.int32)
+    starts = np.zeros(M + 1, np.int32)
+    low = np.zeros(M, np.int32)
+    n = _check(lib.ldpc_step_schedule(C.byref(m), _ip(order), _ip(starts), _ip(low)))
+    return order, starts[:n + 1].copy(), low[:n].copy()
 
 
 @dataclass

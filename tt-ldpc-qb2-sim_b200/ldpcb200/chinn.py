@@ -197,6 +197,62 @@ def row_schedule(mat: Matrix):
     return order, starts
 
 
+def step_schedule(mat: Matrix, dl: int = 3):
+    """The step kernel's schedule (the library's ldpc_step_schedule, restated).
+
+    A row depends on the last earlier row on each of its variables (every pair of rows sharing a
+    variable then keeps its file order).  List scheduling: each step takes up to 32 rows whose
+    predecessors are all scheduled, of one degree class (low: degree <= dl, high otherwise): high when
+    32 high rows are ready, else low when 32 low rows are, else the class with more ready rows (high
+    on a tie); inside a class the rows with the longest chain of dependants first, then file order.
+    Returns (order, starts, low): rows in schedule order, each step's first position followed by M,
+    and 1 for each low step.
+    """
+    import heapq
+    M = mat.M
+    deg = [len(r) for r in mat.rows]
+    last = {}
+    succ = [[] for _ in range(M)]
+    npred = [0] * M
+    for m, r in enumerate(mat.rows):
+        for v in r:
+            v = int(v)
+            p = last.get(v, -1)
+            if p >= 0 and (not succ[p] or succ[p][-1] != m):
+                succ[p].append(m)
+                npred[m] += 1
+            last[v] = m
+    height = [1] * M
+    for m in range(M - 1, -1, -1):
+        for s in succ[m]:
+            height[m] = max(height[m], height[s] + 1)
+    ready = ([], [])  # [0] high, [1] low: heaps of (-height, row)
+
+    def push(m):
+        heapq.heappush(ready[1 if deg[m] <= dl else 0], (-height[m], m))
+
+    for m in range(M):
+        if npred[m] == 0:
+            push(m)
+    order, starts, low = [], [], []
+    while len(order) < M:
+        nh, nl = len(ready[0]), len(ready[1])
+        c = 0 if nh >= 32 else 1 if nl >= 32 else (1 if nl > nh else 0)
+        if not ready[c]:
+            c = 1 - c
+        starts.append(len(order))
+        low.append(c)
+        step = [heapq.heappop(ready[c])[1] for _ in range(min(32, len(ready[c])))]
+        order.extend(step)
+        for m in step:
+            for s in succ[m]:
+                npred[s] -= 1
+                if npred[s] == 0:
+                    push(s)
+    starts.append(M)
+    return order, starts, low
+
+
 def conflict_free_runs(mat: Matrix) -> List[int]:
     """Greedy split of the serial row order into runs of consecutive rows that share no variable.
 
