@@ -1,10 +1,9 @@
 // Step kernel for a general parity-check matrix (any .chinn / .chinn.out file, the reference's serial
 // row order kept where rows share a variable) and its host side.
 //
-// The schedule is the warp kernel's (general_schedule in general.cu: steps of at most 32 rows that
-// share no variable, every pair of rows sharing one in file order), but each step is padded to 32
-// rows so that lane j always takes row j of the step, and every row is padded to the kernel's degree
-// bound DT: a lane without a row and an edge past its row's degree point at a dummy posterior slot
+// Steps of at most 32 rows that share no variable, every pair of rows sharing one in file order (as
+// in the warp kernel's general_schedule), each padded to 32 rows so that lane j always takes row j of
+// the step, and every row is padded to the kernel's degree bound DT: a lane without a row and an edge past its row's degree point at a dummy posterior slot
 // (index N) holding the largest finite value.  Such an edge is never a row's minimum, a min* step with
 // it returns the other operand, its sign is +, and the value it writes back rounds to itself, so the
 // padded rows update exactly like the real ones (row_update's PAD case) with no per-edge predicate
@@ -13,11 +12,14 @@
 // One CTA = one warp = one frame slot, so the frame's posteriors start at shared-memory offset 0 and
 // the column table holds byte offsets that are the shared-memory addresses themselves.  Variables
 // sit in slots chosen against bank conflicts (relabel_slots), which only the channel writes and the
-// posterior output look up.  Per step a
-// lane reads its row's byte offsets (DT 32-bit words, laid out [step][word group][lane] so that every
-// load of the warp is contiguous) and its row's check messages from a global scratch laid out
-// [slot][step][word][lane] (coalesced 4-byte words); both for the next step are loaded while the
-// current step's row is updated.  The messages of all resident slots stay mostly in L2.
+// posterior output look up.  Per step a lane reads its row's byte offsets (DT 32-bit words, laid out
+// [step][word group][lane] so that every load of the warp is contiguous) and its row's check
+// messages from a global scratch laid out [slot][step][word][lane] (coalesced 4-byte words); both for
+// the next step are loaded while the current step's row is updated.  The messages of all resident
+// slots stay mostly in L2.
+//
+// The schedule is the step kernel's own (step_schedule below): steps of one degree class, so that a
+// step of rows of degree <= DT/2 runs the row body of DT/2 edges.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
