@@ -174,7 +174,7 @@ def test_circulant_tile_slices_decode_exactly_h():
 
 
 def test_fixed_table_header_is_current():
-    """csrc/ar4ja_fixed_tables.h (the layer descriptors compiled into the K = 16384 layout-5 kernels)
+    """csrc/ar4ja_fixed_tables.h (the layer descriptors compiled into the layout-5 kernels)
     is what ldpcb200.fixed_tables writes from the makeH construction."""
     from ldpcb200 import fixed_tables
     assert fixed_tables.main(["--check"]) == 0

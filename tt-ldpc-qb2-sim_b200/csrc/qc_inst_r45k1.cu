@@ -32,5 +32,10 @@ static const QcEntry qc_r45k1[] = {
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 32),
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 32),
     LDPC_QC_ENTRY_G(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 32),
+    // layout 5: the register-capped shapes with the code's layer descriptors compiled in
+    // (ar4ja_fixed_tables.h entry 3)
+    LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 32, 3),
+    LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 32, 3),
+    LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 32, 3),
 };
 LDPC_QC_REGISTER(qc_r45k1)

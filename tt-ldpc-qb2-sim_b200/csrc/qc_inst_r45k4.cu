@@ -43,6 +43,11 @@ static const QcEntry qc_r45k4[] = {
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 8),
+    // layout 5: the register-capped shapes with the code's layer descriptors compiled in
+    // (ar4ja_fixed_tables.h entry 4)
+    LDPC_QC_ENTRY_GF(128, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 8, 4),
+    LDPC_QC_ENTRY_GF(128, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8, 4),
+    LDPC_QC_ENTRY_GF(128, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 8, 4),
     // the weighted decoders in the same layout (per-edge and per-row weights)
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_BF16, ALGO_WAMIN, false, false, 8),
     LDPC_QC_ENTRY_G(128, 18, 1, 1, STORE_FP16, ALGO_WAMIN, false, false, 8),

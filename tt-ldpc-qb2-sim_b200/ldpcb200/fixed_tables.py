@@ -1,4 +1,5 @@
-"""Layer descriptors compiled into the K = 16384 global-message kernels (csrc/ar4ja_fixed_tables.h).
+"""Layer descriptors compiled into the global-message kernels (csrc/ar4ja_fixed_tables.h): the K = 16384
+codes and the degree-18 rate-4/5 codes at K = 1024 and 4096.
 
 The QC kernel reads each edge's column block offset and circulant shift from its launch parameters
 (the constant bank); with the descriptors of a known code compiled in, they become immediate
@@ -18,7 +19,7 @@ from typing import List, Tuple
 
 from . import ar4ja
 
-CODES = ((16384, "1/2"), (16384, "2/3"), (16384, "4/5"))
+CODES = ((16384, "1/2"), (16384, "2/3"), (16384, "4/5"), (1024, "4/5"), (4096, "4/5"))
 LAYERS, DMAX = 12, 18
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "csrc", "ar4ja_fixed_tables.h")
 
