@@ -183,8 +183,9 @@ int ldpc_snr_bins(ldpc_handle* h, uint64_t* out);
  * 1 = in global memory (codes too large for the register file), 2 = in registers, with each
  * thread's column offsets precomputed in shared memory, 5 = as 1 with the code's layer descriptors
  * compiled into the kernel (built for the K = 16384 AR4JA codes and the rate-4/5 codes at K = 1024
- * and 4096, in makeH order, offered only when the matrix's descriptors are exactly those; layouts 3
- * and 4 are the general kernels').  All zero restores the default.
+ * and 4096, in makeH order, offered only when the matrix's descriptors are exactly those), 6 = as 0
+ * with the descriptors compiled in (rate 1/2, K = 1024); layouts 3 and 4 are the general kernels'.
+ * All zero restores the default.
  * LDPC_ENOTSUP if the shape is not built for this code.  Used by the autotuner
  * (ldpcb200.capi.Decoder.autotune).  Options with no QC variant built (e.g. clips on a K = 16384
  * code) run on the general kernel. */

@@ -366,6 +366,25 @@ def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
     assert lo <= r.bit_errors <= hi, (ebn0, r.bit_errors / bits, p)
 
 
+@pytest.mark.parametrize("storage", ["fp32", "bf16", "fp16"])
+def test_every_r12k1_shape_equals_default(gpu, storage):
+    """Every built launch shape of the headline code (register caps, paired frames, the offset table,
+    layout 6 with the descriptors compiled in) tallies what the default shape tallies."""
+    c = ar4ja.make_code(1024, "1/2")
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.5)
+    with capi.Decoder.from_code(c, 0) as dec:
+        shapes = dec.shapes(storage)
+        assert any(sh[3] == 6 for sh in shapes), shapes
+        p = dec.params(mu=mu, sigma=sigma, seed=6, n_frames=20000, max_iter=60, storage=storage)
+        base = dec.run_chunk(p)
+        for sh in shapes:
+            dec.set_launch_shape(*sh, storage=storage)
+            r = dec.run_chunk(p)
+            dec.set_launch_shape(0, 0, 0, 0, storage=storage)
+            for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters", "bit_errors_sq"):
+                assert getattr(r, k) == getattr(base, k), (sh, k)
+
+
 def test_sim_cli_long_run_picks_a_shape_and_keeps_the_tallies(tmp_path):
     """The drop-in binary's engine times the built launch shapes before a long run (2^22 frames) and
     reports the choice; the tallies equal a run with the default shape (shapes change only speed)."""

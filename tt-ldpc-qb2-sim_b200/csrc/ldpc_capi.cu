@@ -339,7 +339,7 @@ extern "C" int64_t ldpc_launch_param_bytes(const ldpc_handle* h) {
 }
 
 static const void* find_shape(const ldpc_handle* h, int storage, int algo, int clip, int ext, int R, int F, int B, int G) {
-    if (G == 5 && h->fix < 0) return nullptr;  // compiled-in descriptors of another code
+    if ((G == 5 || G == 6) && h->fix < 0) return nullptr;  // compiled-in descriptors of another code
     return find_qc(QcKey{h->Z, h->D, R, F, storage, algo, clip, ext, B, G});
 }
 
@@ -355,7 +355,7 @@ static bool default_shape(const ldpc_handle* h, int storage, int algo, int clip,
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
             if (k.Z == h->Z && k.D == h->D && k.mode == storage && k.algo == algo && k.clip == clip && k.ext == ext &&
-                (k.G != 5 || h->fix >= 0)) {
+                ((k.G != 5 && k.G != 6) || h->fix >= 0)) {
                 s[0] = k.R; s[1] = k.F; s[2] = k.B; s[3] = k.G;
                 return true;
             }
@@ -455,7 +455,7 @@ static bool general_shape_ok(const ldpc_handle* h, int R, int F, int B, int G) {
 
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 5)
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 6)
         return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
@@ -515,7 +515,7 @@ extern "C" int ldpc_list_shapes_algo(const ldpc_handle* h, int storage, int algo
         for (int i = 0; i < t->count; ++i) {
             const QcKey& k = t->entries[i].key;
             if (k.Z != h->Z || k.D != h->D || k.mode != storage || k.algo != algo || k.clip || k.ext) continue;
-            if (k.G == 5 && h->fix < 0) continue;
+            if ((k.G == 5 || k.G == 6) && h->fix < 0) continue;
             if (n < max_shapes) {
                 shapes[4 * n] = k.R;
                 shapes[4 * n + 1] = k.F;

@@ -577,8 +577,8 @@ __device__ __forceinline__ int qc_shift(const QcParams& p, int l, int e) {
 // registers, for codes whose rows per thread times degrees exceed the register file (K = 16384).
 // OT: the column offset table above, built once per CTA in shared memory after the hard-decision
 // words (T * (12 + 8 D) words); one row per thread.
-// FIX: >= 0 for the descriptors of a known code compiled in (global-message kernels of the K = 16384
-// codes; the host offers them only for a matrix whose descriptors are those).
+// FIX: >= 0 for the descriptors of a known code compiled in (layouts 5 and 6; the host offers them
+// only for a matrix whose descriptors are those).
 template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false,
           bool RG = false, bool OT = false, int FIX = -1>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                   "paired mode: two slots, one row per thread, 16-bit messages, Approximate-Min*, no clips");
     using RE = typename RTraits<MODE>::T;
     static_assert(!OT || (!PAIR && !RG && R == 1), "the offset table is built for one row per thread");
-    static_assert(FIX < 0 || (RG && FIX < QC_FIXED_COUNT), "compiled-in descriptors: global-message kernels");
+    static_assert(FIX < 0 || (!OT && !PAIR && FIX < QC_FIXED_COUNT), "compiled-in descriptors: no offset table");
     constexpr bool CIRC = ALGO == ALGO_CIRC;
     static_assert(!CIRC || (D == 6 && !CLIP && !PAIR), "the circulant engine's decoder: degrees 3 and 6, no clips");
     using SV = SlotView<MODE, PAIR>;

@@ -10,7 +10,8 @@ struct QcKey {
     int Z, D, R, F, mode, algo, clip, ext, B;  // B: min resident CTAs per SM (register cap), 0 = none
     int G;                                     // layout: 0 registers, 1 messages in global memory (RG
                                                // kernel), 2 registers + column offset table (OT),
-                                               // 5 as 1 with a known code's descriptors compiled in
+                                               // 5 as 1 with a known code's descriptors compiled in,
+                                               // 6 as 0 with them compiled in
     // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
     // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
@@ -50,6 +51,12 @@ const QcTable* qc_tables();
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 5},                                \
      reinterpret_cast<const void*>(                                            \
          &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true, false, FIX>)}
+
+// Layout 6: messages in registers with the layer descriptors of fixed-table code FIX compiled in.
+#define LDPC_QC_ENTRY_RF(Z, D, R, F, MODE, ALGO, CLIP, EXT, B, FIX)           \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 6},                                \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, false, false, FIX>)}
 
 #define LDPC_QC_ENTRY_OT(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                 \
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 2},                                \

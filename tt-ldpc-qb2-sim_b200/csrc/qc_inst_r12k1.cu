@@ -51,6 +51,12 @@ static const QcEntry qc_r12k1[] = {
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, true, 0),
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, true, 0),
     LDPC_QC_ENTRY_OT(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, true, 0),
+    // layout 6: messages in registers, the code's layer descriptors compiled in (no offset table)
+    LDPC_QC_ENTRY_RF(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0, 5),
+    LDPC_QC_ENTRY_RF(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 5, 5),
+    LDPC_QC_ENTRY_RF(128, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 6, 5),
+    LDPC_QC_ENTRY_RF(128, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 8, 5),
+    LDPC_QC_ENTRY_RF(128, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 6, 5),
     // weighted Approximate-Min* (trained weights, LDPC_ALGO_WAMIN): simulation and caller-supplied LLRs
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP32, ALGO_WAMIN, false, false),
     LDPC_QC_ENTRY(128, 6, 1, 1, STORE_FP16, ALGO_WAMIN, false, false),
