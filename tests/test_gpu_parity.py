@@ -366,16 +366,21 @@ def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
     assert lo <= r.bit_errors <= hi, (ebn0, r.bit_errors / bits, p)
 
 
-@pytest.mark.parametrize("storage", ["fp32", "bf16", "fp16"])
-def test_every_r12k1_shape_equals_default(gpu, storage):
-    """Every built launch shape of the headline code (register caps, paired frames, the offset table,
-    layout 6 with the descriptors compiled in) tallies what the default shape tallies."""
-    c = ar4ja.make_code(1024, "1/2")
-    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.5)
+@pytest.mark.parametrize("K,rate,storage,frames", [(1024, "1/2", "fp32", 20000), (1024, "1/2", "bf16", 20000),
+                                                     (1024, "1/2", "fp16", 20000), (1024, "2/3", "bf16", 20000),
+                                                     (4096, "1/2", "fp32", 4000), (4096, "1/2", "bf16", 4000),
+                                                     (4096, "1/2", "fp16", 4000), (4096, "2/3", "fp32", 4000),
+                                                     (4096, "2/3", "bf16", 4000), (4096, "2/3", "fp16", 4000)])
+def test_every_shape_equals_default(gpu, K, rate, storage, frames):
+    """Every built launch shape of the codes with layout 6 (register caps, paired frames, the offset
+    table, and layout 6: messages in registers with the descriptors compiled in) tallies what the
+    default shape tallies."""
+    c = ar4ja.make_code(K, rate)
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, 1.5 if rate == "1/2" else 2.3)
     with capi.Decoder.from_code(c, 0) as dec:
         shapes = dec.shapes(storage)
         assert any(sh[3] == 6 for sh in shapes), shapes
-        p = dec.params(mu=mu, sigma=sigma, seed=6, n_frames=20000, max_iter=60, storage=storage)
+        p = dec.params(mu=mu, sigma=sigma, seed=6, n_frames=frames, max_iter=60, storage=storage)
         base = dec.run_chunk(p)
         for sh in shapes:
             dec.set_launch_shape(*sh, storage=storage)

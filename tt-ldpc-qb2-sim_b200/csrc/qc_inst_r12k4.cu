@@ -25,5 +25,9 @@ static const QcEntry qc_r12k4[] = {
     LDPC_QC_ENTRY_OT(512, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(512, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(512, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
+    // layout 6: the code's descriptors compiled in, no offset table (its 120 KB held one CTA per SM)
+    LDPC_QC_ENTRY_RF(512, 6, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 1, 6),
+    LDPC_QC_ENTRY_RF(512, 6, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 2, 6),
+    LDPC_QC_ENTRY_RF(512, 6, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 2, 6),
 };
 LDPC_QC_REGISTER(qc_r12k4)

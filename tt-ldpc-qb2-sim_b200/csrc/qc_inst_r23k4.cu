@@ -21,5 +21,9 @@ static const QcEntry qc_r23k4[] = {
     LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 0),
     LDPC_QC_ENTRY_OT(256, 10, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 0),
+    // layout 6: the code's descriptors compiled in, no offset table
+    LDPC_QC_ENTRY_RF(256, 10, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 2, 7),
+    LDPC_QC_ENTRY_RF(256, 10, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 2, 7),
+    LDPC_QC_ENTRY_RF(256, 10, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 3, 7),
 };
 LDPC_QC_REGISTER(qc_r23k4)

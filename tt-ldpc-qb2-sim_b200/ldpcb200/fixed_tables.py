@@ -19,7 +19,8 @@ from typing import List, Tuple
 
 from . import ar4ja
 
-CODES = ((16384, "1/2"), (16384, "2/3"), (16384, "4/5"), (1024, "4/5"), (4096, "4/5"), (1024, "1/2"))
+CODES = ((16384, "1/2"), (16384, "2/3"), (16384, "4/5"), (1024, "4/5"), (4096, "4/5"), (1024, "1/2"),
+         (4096, "1/2"), (4096, "2/3"), (1024, "2/3"))
 LAYERS, DMAX = 12, 18
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "csrc", "ar4ja_fixed_tables.h")
 
