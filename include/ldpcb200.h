@@ -184,7 +184,9 @@ int ldpc_snr_bins(ldpc_handle* h, uint64_t* out);
  * thread's column offsets precomputed in shared memory, 5 = as 1 with the code's layer descriptors
  * compiled into the kernel (built for the K = 16384 AR4JA codes and the rate-4/5 codes at K = 1024
  * and 4096, in makeH order, offered only when the matrix's descriptors are exactly those), 6 = as 0
- * with the descriptors compiled in (rates 1/2 and 2/3 at K = 1024 and 4096); layouts 3 and 4 are the
+ * with the descriptors compiled in (rates 1/2 and 2/3 at K = 1024 and 4096), 7 = as 1 with the
+ * degree-D layers in a loop that is not unrolled, its descriptors read by layer index (rate 4/5 at
+ * K = 1024 and 4096, rate 2/3 at K = 1024: any matrix of that shape); layouts 3 and 4 are the
  * general kernels'.
  * All zero restores the default.
  * LDPC_ENOTSUP if the shape is not built for this code.  Used by the autotuner

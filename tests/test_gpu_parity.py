@@ -324,8 +324,9 @@ def test_degree18_fp32_global_messages_equal_general_kernel(gpu, K):
                                               (4096, "4/5", ("bf16", "fp16", "fp32"))])
 def test_register_capped_global_message_shapes_equal_default(gpu, K, rate, storages):
     """The register-capped global-message shapes (two CTAs per SM for K = 16384, 64 registers for
-    the degree-18 rate-4/5 codes) and the layout-5 shapes (the code's descriptors compiled in; every
-    one of these codes has some) tally exactly what the default shape tallies on the same frames."""
+    the degree-18 rate-4/5 codes), the layout-5 shapes (the code's descriptors compiled in; every
+    one of these codes has some) and the layout-7 shapes (the degree-18 layers in a loop that is not
+    unrolled, K = 1024 and 4096) tally exactly what the default shape tallies on the same frames."""
     from ldpcb200 import threshold
     c = ar4ja.make_code(K, rate)
     mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db(rate) + 0.5)
@@ -334,6 +335,7 @@ def test_register_capped_global_message_shapes_equal_default(gpu, K, rate, stora
             shapes = dec.shapes(st)
             assert rate == "1/2" or any(sh[2] > 0 and sh[3] == 1 for sh in shapes), (st, shapes)
             assert any(sh[3] == 5 for sh in shapes), (st, shapes)
+            assert K == 16384 or any(sh[3] == 7 for sh in shapes), (st, shapes)
             p = dec.params(mu=mu, sigma=sigma, seed=4, n_frames=600 if K == 16384 else 2000, max_iter=60,
                            storage=st)
             base = dec.run_chunk(p)

@@ -377,8 +377,10 @@ def test_weighted_requires_weights_and_rejects_clips(gpu):
 
 
 @pytest.mark.parametrize("K,rate,storage", [(1024, "1/2", "fp32"), (1024, "1/2", "fp16"), (4096, "4/5", "fp16"),
-                                            (4096, "4/5", "bf16")])
+                                            (4096, "4/5", "bf16"), (4096, "4/5", "fp32")])
 def test_weighted_offset_table_shapes_equal_default(gpu, K, rate, storage):
+    """The weighted decoder's offset-table shapes (layout 2) and, for the degree-18 code, its
+    global-message shapes with the rolled layer loop (layout 7) tally what the default shape tallies."""
     code = ar4ja.make_code(K, rate)
     a, b = _params(code, 20, 3, torch.float32)
     mu, sigma = capi.channel_mu_sigma(code.N, code.n_checks, code.P, 2.0 if rate == "1/2" else 3.2)
@@ -387,8 +389,8 @@ def test_weighted_offset_table_shapes_equal_default(gpu, K, rate, storage):
         p = dec.params(mu=mu, sigma=sigma, seed=5, n_frames=2000 if K == 1024 else 300, max_iter=20,
                        storage=storage, algo=capi.ALGO_WAMIN)
         base = dec.run_chunk(p)
-        shapes = [s_ for s_ in dec.shapes(storage, capi.ALGO_WAMIN) if s_[3] == 2]
-        assert shapes
+        shapes = [s_ for s_ in dec.shapes(storage, capi.ALGO_WAMIN) if s_[3] in (2, 7)]
+        assert shapes and (rate != "4/5" or any(s_[3] == 7 for s_ in shapes)), shapes
         for sh in shapes:
             dec.set_launch_shape(*sh, storage=storage)
             r = dec.run_chunk(p)
@@ -414,7 +416,9 @@ def _row_uniform_params(code, T, seed):
 @pytest.mark.parametrize("K,rate,storage,shape", [(1024, "1/2", "fp32", None), (1024, "1/2", "fp32", (1, 1, 5, 2)),
                                                   (1024, "1/2", "fp16", (1, 1, 6, 2)), (1024, "1/2", "bf16", None),
                                                   (4096, "4/5", "fp16", (1, 1, 0, 2)), (4096, "4/5", "bf16", (1, 1, 8, 1)),
-                                                  (4096, "4/5", "fp32", (1, 1, 8, 1))])
+                                                  (4096, "4/5", "fp32", (1, 1, 8, 1)),
+                                                  (4096, "4/5", "fp32", (1, 1, 6, 7)),
+                                                  (4096, "4/5", "bf16", (1, 1, 6, 7))])
 def test_row_weights_equal_per_edge_weights(gpu, K, rate, storage, shape):
     """Weights with one class per protograph check row run on the per-row kernels (the pair applied
     to the row's two magnitudes); the same values given per edge run on the per-edge kernels.  The two

@@ -455,7 +455,7 @@ static bool general_shape_ok(const ldpc_handle* h, int R, int F, int B, int G) {
 
 extern "C" int ldpc_set_launch_shape(ldpc_handle* h, int storage, int R, int F, int B, int G) {
     if (!h) return fail(LDPC_EINVAL, "handle is NULL");
-    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 6)
+    if (storage < -1 || storage > 2 || R < 0 || F < 0 || B < 0 || G < 0 || G > 7)
         return fail(LDPC_EINVAL, "bad shape storage=%d R=%d F=%d B=%d G=%d", storage, R, F, B, G);
     const int lo = storage < 0 ? 0 : storage, hi = storage < 0 ? 2 : storage;
     const bool reset = R == 0 && F == 0 && B == 0 && G == 0;
@@ -686,7 +686,7 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     out->block = T;
     out->smem = smem;
     if (grid == 0) return 0;
-    if (G == 1 || G == 5) {
+    if (G == 1 || G == 5 || G == 7) {
         int rc;
         const size_t rsz = p->storage == LDPC_STORE_FP32 ? 4 : 2;
         if ((rc = ensure_cap(&h->d_rmsg, &h->rmsg_cap, grid * F * (size_t)qp.slot_elems * rsz))) return rc;

@@ -579,8 +579,12 @@ __device__ __forceinline__ int qc_shift(const QcParams& p, int l, int e) {
 // words (T * (12 + 8 D) words); one row per thread.
 // FIX: >= 0 for the descriptors of a known code compiled in (layouts 5 and 6; the host offers them
 // only for a matrix whose descriptors are those).
+// ROLL (layout 7, global messages only): the eight degree-D layers run as one loop that is not
+// unrolled, each row's descriptors read from the kernel parameters by layer index.  The unrolled
+// body of a degree-18 code is tens of KB of instructions; with one-warp CTAs whose warps are
+// each at a different point of it, the instruction fetch stalls the SM.
 template <int Z, int D, int R, int F, int MODE, int ALGO, bool CLIP, bool EXT, int B = 0, bool PAIR = false,
-          bool RG = false, bool OT = false, int FIX = -1>
+          bool RG = false, bool OT = false, int FIX = -1, bool ROLL = false>
 __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_constant__ QcParams p) {
     constexpr int T = Z / R;
     constexpr int W = Z / 32;  // 32-bit words per Z-bit block vector
@@ -592,6 +596,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
     static_assert(!OT || (!PAIR && !RG && R == 1), "the offset table is built for one row per thread");
     static_assert(FIX < 0 || (!OT && !PAIR && FIX < QC_FIXED_COUNT), "compiled-in descriptors: no offset table");
     constexpr bool CIRC = ALGO == ALGO_CIRC;
+    static_assert(!ROLL || (RG && FIX < 0 && !CIRC), "the rolled layer loop: global messages, parameter descriptors");
     static_assert(!CIRC || (D == 6 && !CLIP && !PAIR), "the circulant engine's decoder: degrees 3 and 6, no clips");
     using SV = SlotView<MODE, PAIR>;
     using LT = LTraits<MODE>;
@@ -733,7 +738,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 else ot_load<QC_DEG_LOW, T>(sOT, tid, offs[0]);
             }
 #pragma unroll
-            for (int l = 0; l < QC_LAYERS; ++l) {
+            for (int l = 0; l < (ROLL ? 4 : QC_LAYERS); ++l) {
                 const int ly = CIRC ? (l + 4) % QC_LAYERS : l;        // the layer updated at step l
                 const int ly_next = CIRC ? (l + 5) % QC_LAYERS : l + 1;
                 const float2* wl[F];
@@ -806,6 +811,31 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                     }
                 }
                 __syncthreads();
+            }
+            if constexpr (ROLL) {
+#pragma unroll 1
+                for (int ly = 4; ly < QC_LAYERS; ++ly) {
+                    const float2* wl[F];
+#pragma unroll
+                    for (int f = 0; f < F; ++f)
+                        wl[f] = ALGO == ALGO_WAMIN ? wt[f] + qc_edge_slot(ly, 0, D)
+                                                   : (ALGO == ALGO_WROW ? wt[f] + ly : nullptr);
+#pragma unroll
+                    for (int rho = 0; rho < R; ++rho) {
+                        const int j = tid + rho * T;
+                        int idx[D];
+#pragma unroll
+                        for (int e = 0; e < D; ++e) idx[e] = p.blk_off[ly][e] + ((j + p.shift[ly][e]) & (Z - 1));
+                        RowMsgGlobal<D, MODE> rm[F];
+#pragma unroll
+                        for (int f = 0; f < F; ++f)
+                            rm[f] = RowMsgGlobal<D, MODE>{
+                                reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
+                                    p.layer_off[ly] + j, Z};
+                        row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
+                    }
+                    __syncthreads();
+                }
             }
 #pragma unroll
             for (int f = 0; f < F; ++f) it[f] += (act >> f) & 1u;

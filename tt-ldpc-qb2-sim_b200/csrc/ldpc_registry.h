@@ -11,7 +11,8 @@ struct QcKey {
     int G;                                     // layout: 0 registers, 1 messages in global memory (RG
                                                // kernel), 2 registers + column offset table (OT),
                                                // 5 as 1 with a known code's descriptors compiled in,
-                                               // 6 as 0 with them compiled in
+                                               // 6 as 0 with them compiled in, 7 as 1 with the
+                                               // degree-D layers in a loop not unrolled
     // F = 2 with 16-bit storage, Approximate-Min*, no clips is the paired kernel (two interleaved
     // slots per thread, packed f32x2 arithmetic).
     bool operator==(const QcKey& o) const {
@@ -57,6 +58,12 @@ const QcTable* qc_tables();
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 6},                                \
      reinterpret_cast<const void*>(                                            \
          &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, false, false, FIX>)}
+
+// Layout 7: the global-message kernel with its degree-D layers in a loop that is not unrolled.
+#define LDPC_QC_ENTRY_GR(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                 \
+    {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 7},                                \
+     reinterpret_cast<const void*>(                                            \
+         &::ldpcb200::qc_decode_kernel<Z, D, R, F, MODE, ALGO, CLIP, EXT, B, false, true, false, -1, true>)}
 
 #define LDPC_QC_ENTRY_OT(Z, D, R, F, MODE, ALGO, CLIP, EXT, B)                 \
     {{Z, D, R, F, MODE, ALGO, CLIP, EXT, B, 2},                                \

@@ -37,5 +37,16 @@ static const QcEntry qc_r45k1[] = {
     LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 32, 3),
     LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 32, 3),
     LDPC_QC_ENTRY_GF(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 32, 3),
+    // layout 7: the eight degree-18 layers in a loop that is not unrolled.  The unrolled body does
+    // not fit the instruction cache, and with one-warp CTAs each warp is somewhere else in it (ncu:
+    // 9 no-instruction stalls per issue, issue 46 %).  Rolled, at 16-24 CTAs per SM (80-112
+    // registers, no 64-register spills, a message scratch that stays in L2): fp32 23.1 -> 34.5,
+    // bf16 21.3 -> 30.9 M frames/s at threshold + 1.25 dB.
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 24),
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 20),
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_FP32, ALGO_AMIN, false, false, 16),
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 24),
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_BF16, ALGO_AMIN, false, false, 16),
+    LDPC_QC_ENTRY_GR(32, 18, 1, 1, STORE_FP16, ALGO_AMIN, false, false, 16),
 };
 LDPC_QC_REGISTER(qc_r45k1)
