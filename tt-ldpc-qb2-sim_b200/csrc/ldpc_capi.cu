@@ -663,8 +663,8 @@ static int prepare_qc(ldpc_handle* h, const ldpc_run_params* p, bool ext, uint32
     const int T = h->Z / R;
     int32_t off = 0;
     for (int l = 0; l < QC_LAYERS; ++l) {
-        qp.layer_off[l] = off;
-        off += h->Z * (l < 4 ? QC_DEG_LOW : h->D);
+        qp.layer_off[l] = off;  // the global-message layout keeps edges in pairs: odd degrees padded
+        off += h->Z * (((l < 4 ? QC_DEG_LOW : h->D) + 1) & ~1);
     }
     qp.slot_elems = off;
     const size_t esz = p->storage == LDPC_STORE_BF16 ? 2 : 4;

@@ -22,6 +22,7 @@
 // frame counter: early-retire with slot refill, so fast and slow frames never wait for each other.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include "ar4ja_fixed_tables.h"
 #include "ldpc_device.cuh"
 
@@ -55,8 +56,8 @@ struct QcParams {
     int32_t hist_bins;
     unsigned int* work;                   // frame claim counter, zero at launch
     void* r_base;                         // messages in global memory (RG kernels): [slot][edges]
-    int32_t layer_off[QC_LAYERS];         // element offset of layer l's messages in a slot ([edge][row])
-    int32_t slot_elems;                   // messages per slot (edges of the code)
+    int32_t layer_off[QC_LAYERS];         // element offset of layer l's messages in a slot ([pair][row])
+    int32_t slot_elems;                   // message elements per slot (edges, odd degrees padded)
     float ebn0_lo, ebn0_hi;               // per-frame Eb/N0 range in dB (used when hi > lo)
     float rate;                           // (N - M) / (N - P), for the per-frame mu and sigma
     unsigned long long* snr_bins;         // [4][SNR_BINS]: frames, frame errors, bit errors, iterations
@@ -167,17 +168,48 @@ template <int d> struct RowMsg<d, STORE_FP32> {
     }
 };
 
-// Messages of one row kept in global memory (RG kernels): edge e at p[e * stride].  A slot's
-// messages are laid out [layer][edge][row], so the threads of a CTA touch consecutive addresses.
+// Messages of one row kept in global memory (RG kernels).  Edges 2k and 2k+1 of a row share one
+// 32-bit word (16-bit storage) or one float2 (fp32), pair k at w[k * stride]: a slot's messages are
+// laid out [layer][pair][row], so the threads of a CTA (consecutive rows) touch consecutive words
+// and a row's two edges cost one load and one store.  An odd degree's last pair holds a zero.
 template <int d, int MODE> struct RowMsgGlobal {
-    typename RTraits<MODE>::T* p;
+    using W = typename std::conditional<MODE == STORE_FP32, float2, uint32_t>::type;
+    W* w;
     int stride;
-    __device__ __forceinline__ float get(int e) const { return RTraits<MODE>::ld(p + (size_t)e * stride); }
-    __device__ __forceinline__ void set2(int e, float a, float b) {
-        RTraits<MODE>::st(p + (size_t)e * stride, a);
-        if (e + 1 < d) RTraits<MODE>::st(p + (size_t)(e + 1) * stride, b);
+    __device__ __forceinline__ float get(int e) const {
+        const W x = w[(e >> 1) * stride];
+        if constexpr (MODE == STORE_FP32) {
+            return (e & 1) ? x.y : x.x;
+        } else if constexpr (MODE == STORE_BF16) {
+            return (e & 1) ? __uint_as_float(x & 0xFFFF0000u) : __uint_as_float(x << 16);
+        } else {
+            const __half2 h = *reinterpret_cast<const __half2*>(&x);
+            return (e & 1) ? __high2float(h) : __low2float(h);
+        }
+    }
+    __device__ __forceinline__ void set2(int e, float a, float b) {  // e even: edges e and e+1
+        W x;
+        if constexpr (MODE == STORE_FP32) {
+            x = make_float2(a, b);
+        } else if constexpr (MODE == STORE_BF16) {
+            __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+            x = *reinterpret_cast<uint32_t*>(&v);
+        } else {
+            a = fminf(fmaxf(a, -65504.0f), 65504.0f);
+            b = fminf(fmaxf(b, -65504.0f), 65504.0f);
+            __half2 v = __floats2half2_rn(a, b);
+            x = *reinterpret_cast<uint32_t*>(&v);
+        }
+        w[(e >> 1) * stride] = x;
     }
 };
+// Row j of layer ly in message slot `slot` (Z rows per layer).
+template <int d, int MODE, int Z>
+__device__ __forceinline__ RowMsgGlobal<d, MODE> rg_row(const QcParams& p, size_t slot, int ly, int j) {
+    using W = typename RowMsgGlobal<d, MODE>::W;
+    auto* base = reinterpret_cast<typename RTraits<MODE>::T*>(p.r_base) + slot * p.slot_elems + p.layer_off[ly];
+    return RowMsgGlobal<d, MODE>{reinterpret_cast<W*>(base) + j, Z};
+}
 
 // Update one row of degree d for the F slots (all slots in lockstep; slot f's L array at
 // sL + f*lstride).  idx[e]: the row's column indices.
@@ -769,9 +801,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                             RowMsgGlobal<QC_DEG_LOW, MODE> rm[F];
 #pragma unroll
                             for (int f = 0; f < F; ++f)
-                                rm[f] = RowMsgGlobal<QC_DEG_LOW, MODE>{
-                                    reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
-                                        p.layer_off[ly] + j, Z};
+                                rm[f] = rg_row<QC_DEG_LOW, MODE, Z>(p, (size_t)blockIdx.x * F + f, ly, j);
                             if constexpr (CIRC) row_update_circ<QC_DEG_LOW, MODE, F>(idx, sL, lstride, rm, cr);
                             else row_update<QC_DEG_LOW, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
@@ -795,9 +825,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                             RowMsgGlobal<D, MODE> rm[F];
 #pragma unroll
                             for (int f = 0; f < F; ++f)
-                                rm[f] = RowMsgGlobal<D, MODE>{
-                                    reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
-                                        p.layer_off[ly] + j, Z};
+                                rm[f] = rg_row<D, MODE, Z>(p, (size_t)blockIdx.x * F + f, ly, j);
                             if constexpr (CIRC) row_update_circ<D, MODE, F>(idx, sL, lstride, rm, cr);
                             else row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                         } else if constexpr (PAIR)
@@ -829,9 +857,7 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                         RowMsgGlobal<D, MODE> rm[F];
 #pragma unroll
                         for (int f = 0; f < F; ++f)
-                            rm[f] = RowMsgGlobal<D, MODE>{
-                                reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems +
-                                    p.layer_off[ly] + j, Z};
+                            rm[f] = rg_row<D, MODE, Z>(p, (size_t)blockIdx.x * F + f, ly, j);
                         row_update<D, MODE, ALGO, CLIP, F>(idx, sL, lstride, rm, r_cap, lp_cap, wl);
                     }
                     __syncthreads();
