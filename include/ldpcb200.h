@@ -226,8 +226,8 @@ int64_t ldpc_launch_param_bytes(const ldpc_handle* h);
  * more than that for one CTA of frame slots (4 slots, or 1 when a frame's posteriors are too large
  * for 4 to share a CTA, as in ldpc_decode_llr) is rejected with LDPC_ENOMEM; smaller ones run with as
  * many frame slots as fit.  Any n_frames >= 0 is accepted (decoded in launches of at most 2^31
- * frames).  The first call on a device looks the array up on that device (make that first call
- * before any stream capture).  Every call reuses the same array: calls whose work can overlap on the
+ * frames).  The first call on a device looks the array up on that device.  Every call reuses the
+ * same array: calls whose work can overlap on the
  * GPU race and must be serialised by the caller.  Each call synchronises `stream` before it returns,
  * so the outputs are ready when it does. */
 int ldpc_decode_llr_static(const ldpc_matrix* h, const ldpc_run_params* p, const float* d_llr,
