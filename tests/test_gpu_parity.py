@@ -348,6 +348,51 @@ def test_register_capped_global_message_shapes_equal_default(gpu, K, rate, stora
                     assert getattr(r, k) == getattr(base, k), (st, sh, k)
 
 
+def _reshifted_rows(code, seed):
+    """The code's row matrix with every circulant shift drawn anew: the same QC shape (layers,
+    column blocks, degrees), other descriptors than the makeH code's."""
+    g = np.random.default_rng(seed)
+    Z = code.Z
+    out = np.full((code.n_checks, max(code.layer_degrees)), -1, np.int32)
+    j = np.arange(Z)
+    for l, lay in enumerate(code.layers):
+        for e, (b, _) in enumerate(lay):
+            out[l * Z:(l + 1) * Z, e] = b * Z + (j + int(g.integers(Z))) % Z
+    return out
+
+
+@pytest.mark.parametrize("rate,storage", [("4/5", "fp32"), ("4/5", "bf16"), ("2/3", "fp32")])
+def test_rolled_layout_serves_any_shifts(gpu, rate, storage):
+    """Layout 7 reads the layer descriptors from the kernel parameters, so a QC matrix of the same
+    shape with other circulant shifts (not the makeH code: no compiled-in layout 5 or 6 for it) runs
+    on it.  Every layout-7 shape tallies what the default shape tallies, and the simulation equals
+    decoding its own exported channel LLRs through ldpc_decode_llr."""
+    from ldpcb200 import threshold
+    c = ar4ja.make_code(1024, rate)
+    rows = _reshifted_rows(c, 11)
+    assert not np.array_equal(rows, c.row_matrix())
+    mu, sigma = capi.channel_mu_sigma(c.N, c.n_checks, c.P, threshold.threshold_db(rate) + 1.0)
+    with capi.Decoder(rows, c.N, c.P, 0) as dec:
+        shapes = dec.shapes(storage)
+        rolled = [sh for sh in shapes if sh[3] == 7]
+        assert rolled and not any(sh[3] in (5, 6) for sh in shapes), shapes
+        p = dec.params(mu=mu, sigma=sigma, seed=9, n_frames=1500, max_iter=60, storage=storage)
+        base = dec.run_chunk(p)
+        for sh in rolled:
+            dec.set_launch_shape(*sh, storage=storage)
+            r = dec.run_chunk(p)
+            for k in ("frames", "bit_errors", "frame_errors", "iter_sum", "unconverged", "max_iters",
+                      "bit_errors_sq"):
+                assert getattr(r, k) == getattr(base, k), (sh, k)
+        dec.set_launch_shape(0, 0, 0, 0, storage=storage)
+        llr = dec.channel_llr(p)
+        _, it, sf, be, tal = dec.decode_llr(llr, p, want_post=False)
+    assert (base.frames, base.bit_errors, base.frame_errors, base.iter_sum, base.unconverged, base.bit_errors_sq) == \
+           (tal.frames, tal.bit_errors, tal.frame_errors, tal.iter_sum, tal.unconverged, tal.bit_errors_sq)
+    _check_tally(tal, it, sf, be)
+    assert 0 < base.iter_sum
+
+
 @pytest.mark.parametrize("ebn0", [0.0, 2.0, 4.0, 6.0, 8.0])
 def test_uncoded_ber_matches_bpsk_theory(dec_r12k1, ebn0):
     """With no decoding iterations the tallies count the channel's own hard-decision errors: BPSK
