@@ -721,7 +721,8 @@ __global__ void __launch_bounds__(Z / R, B) qc_decode_kernel(const __grid_consta
                 it[f] = 0;
                 if (fid[f] == 0xFFFFFFFFu) { act &= ~(1u << f); continue; }
                 act |= 1u << f;
-                if constexpr (RG) {  // each thread clears exactly the messages of its own rows
+                if constexpr (RG) {  // the CTA clears the slot's messages; the barrier that ends the refill
+                                     // makes the zeros visible to each row's owner
                     RE* rs = reinterpret_cast<RE*>(p.r_base) + ((size_t)blockIdx.x * F + f) * p.slot_elems;
                     for (int i = tid; i < p.slot_elems; i += T) rs[i] = RE(0);
                 } else {
